@@ -1,0 +1,359 @@
+"""Benchmark of the B200 GRN evaluator (one JSON line on stdout, rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+                  [--impl ours|reference] [--models M] [--no-cpu-baseline]
+
+A bench step is one pass of the hot path over one batch: every model of the
+workload simulated for all its Euler steps and scored (default workload
+uneven_64x64: 4096 models, 2-8 genes, 1-24 links, 64x64 grid, 2000 steps).
+
+  value   fitness evaluations/s with the packed batch resident on the device:
+          K launches timed with CUDA events on the launching stream, each
+          launch bracketed by its own events; between launches a 256 MiB
+          buffer is written to flush L2 (outside the events).
+  e2e     the same metric through grn_evaluate_batch with host buffers:
+          host compile of the batch, pinned H2D copy, kernel, D2H of the raw
+          errors and host rounding inside the timed region (wall clock,
+          synchronised on both sides).
+  roofline  MUFU (SFU pipe) bound: algorithmic MUFU ops of a launch (lg2 per
+          regulator gene, ex2 + rcp per regulated gene, per cell-step) over
+          the mean launch time, against 16 MUFU/clk/SM x SMs x max SM clock.
+  cpu_baseline  the FP64 oracle (a port of the reference's CPU evaluator) on
+          the host cores, on a bounded sample of the same workload.
+
+--impl reference times the reference's CPU path (the oracle port; the
+reference itself cannot be built here) on the host cores instead.
+Multi-GPU: one process per GPU under torchrun; every rank evaluates its own
+full batch (seeded by rank), so the work per GPU is fixed (weak scaling) and
+no collective touches the data path; timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "grn-gpu-performance_b200"))
+
+import synth  # noqa: E402
+
+SFU_PER_CLK_PER_SM = 16  # MUFU results per clock per SM (lg2/ex2/rcp, FP32)
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def read_profile(workload):
+    """DRAM traffic per launch of the simulation kernel from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "sim_kernel_%s.json" % workload)
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(workload, seed, budget_s=15.0, threads=None):
+    """Times the FP64 oracle on a bounded sample of the workload: one model
+    per host thread per round, full Euler steps, rounds until ~budget_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import binding as oracle  # oracle = the CPU baseline only
+    threads = threads or os.cpu_count() or 1
+    params, batch, init, tgt = synth.workload(workload, seed=seed + 1000,
+                                              n_models=max(threads, 1))
+    t0 = time.perf_counter()
+    oracle.evaluate_batch(params, init, tgt, batch.subset([0]), n_threads=1)
+    t1 = time.perf_counter() - t0
+    rounds = max(1, min(8, int(budget_s / max(t1, 1e-3))))
+    n = threads * rounds
+    params, batch, init, tgt = synth.workload(workload, seed=seed + 1000, n_models=n)
+    t0 = time.perf_counter()
+    oracle.evaluate_batch(params, init, tgt, batch, n_threads=threads)
+    dt = time.perf_counter() - t0
+    cells = params["dim_x"] * params["dim_y"] * params["num_sim_steps"] * n
+    return {"value": n / dt, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": "%d models of %s (full %d steps), %d threads, %.1f s"
+                      % (n, workload, params["num_sim_steps"], threads, dt),
+            "cell_updates_per_s": cells / dt}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU evaluator (oracle port) on the
+    host cores, rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    wl = synth.WORKLOADS[args.workload]
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args.workload, seed=i, budget_s=args.ref_budget, threads=threads)
+        if i >= args.warmup:
+            vals.append(cb)
+    value = statistics.mean(v["value"] for v in vals)
+    line = {
+        "impl": "reference", "metric": "GRN fitness evals/sec", "value": value,
+        "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * statistics.mean(
+            float(v["sample"].split(", ")[-1].split()[0]) for v in vals),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "models": wl["n_models"],
+                   "grid": "%dx%d" % (wl["W"], wl["H"]), "euler_steps": wl["steps"]},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
+                         "sample": vals[-1]["sample"]},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "cell_updates_per_s": statistics.mean(v["cell_updates_per_s"] for v in vals),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="uneven_64x64", choices=sorted(synth.WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--models", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=12.0)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import grn_b200 as grn
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    params, batch, init, tgt = synth.workload(args.workload, seed=args.seed + rank,
+                                              n_models=args.models)
+    n = batch.n_models
+    ev = grn.Evaluator(params, device=local)
+    ev.set_experiments(init, tgt)
+    pk = ev.pack(batch)
+    info = pk.info
+    me = torch.full((n,), 1000.0, dtype=torch.float64, device="cuda")
+    raw = torch.zeros(n, dtype=torch.float64, device="cuda")
+    steps_out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        pk.run(me.data_ptr(), raw.data_ptr(), steps_out.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        launch()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing (value) ----
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    evs = []
+    for i in range(args.steps):
+        flush.fill_(i & 0xff)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier()
+    launch_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(launch_ms))
+    clocks = sampler.stop() if sampler else None
+    steps_run = int(steps_out.sum().item())
+    cells = params["dim_x"] * params["dim_y"]
+
+    # ---- end-to-end through the C ABI with host buffers (e2e) ----
+    e2e_times = []
+    stats = None
+    for i in range(max(1, args.warmup // 2) + args.steps):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        err, rawh, stats = ev.evaluate_batch(batch)
+        t1 = time.perf_counter()
+        if i >= max(1, args.warmup // 2):
+            e2e_times.append(t1 - t0)
+    e2e_s = max_over_ranks(sum(e2e_times))
+    assert np.isfinite(rawh).all()
+    np.testing.assert_array_equal(rawh, raw.cpu().numpy())
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    peaks, peak_kind = read_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    props = torch.cuda.get_device_properties(local)
+    n_sm = props.multi_processor_count
+    mean_ms = statistics.mean(launch_ms)
+    # sfu_ops_per_step sums every model's MUFU ops of one Euler step over the
+    # grid; steps_run / n is the Euler steps each model ran (all equal here:
+    # min_conc_change 0 never stops a simulation early).
+    sfu_ops = info["sfu_ops_per_step"] * (steps_run / max(n, 1))
+    achieved = sfu_ops / (mean_ms / 1000.0) / 1e9
+    peak = SFU_PER_CLK_PER_SM * n_sm * sm_max * 1e6 / 1e9
+    prof = read_profile(args.workload)
+    value = n * world * args.steps / (total_ms / 1000.0)
+    line = {
+        "metric": "GRN fitness evals/sec",
+        "value": value,
+        "unit": "evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": args.workload, "models_per_gpu": n,
+            "grid": "%dx%d" % (params["dim_x"], params["dim_y"]),
+            "genes": "%d-%d" % synth.WORKLOADS[args.workload]["genes"],
+            "links": "%d-%d" % synth.WORKLOADS[args.workload]["links"],
+            "mean_genes": round(info["mean_genes"], 3), "mean_links": round(info["mean_links"], 3),
+            "euler_steps": params["num_sim_steps"], "experiments": int(init.shape[0]),
+            "fitness": ["ref_logthresh", "mse"][params["fitness_kind"]],
+            "state": "fp32, fitness sums fp64",
+            "l2": "256 MiB buffer written between timed launches (outside the launch events)",
+            "schedule": grn.SCHEDULE_NAMES.get(stats["schedule"], stats["schedule"]),
+            "threads_per_block": stats["threads_per_block"], "blocks": stats["blocks"],
+            "parallelism": "independent batch per GPU" if world > 1 else "1 GPU",
+        },
+        "cell_updates_per_s": steps_run * cells * world * args.steps / (total_ms / 1000.0),
+        "e2e": {
+            "value": n * world * args.steps / e2e_s,
+            "unit": "evals/s",
+            "h2d_bytes_per_step": int(stats["h2d_bytes"]),
+            "d2h_bytes_per_step": int(stats["d2h_bytes"]),
+            "host_pack_ms": round(stats["pack_ms"], 3),
+        },
+        "roofline": {
+            "bound": "sfu",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "Gop/s (MUFU lg2/ex2/rcp)",
+            "frac": achieved / peak,
+            "peak_source": "16 MUFU/clk/SM x %d SMs x %.0f MHz (%s sm_max_mhz)" % (
+                n_sm, sm_max, peak_kind),
+            "traffic": prof.get("dram_bytes_per_launch") if prof else None,
+            "kernel": "sim_kernel",
+            "launch_ms": round(mean_ms, 3),
+        },
+        "clocks": clocks,
+        "gpu_launches": args.steps,
+    }
+    if clocks and clocks.get("sm_mhz"):
+        line["roofline"]["frac_at_sampled_clock"] = achieved / (
+            SFU_PER_CLK_PER_SM * n_sm * clocks["sm_mhz"] * 1e6 / 1e9)
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.workload, args.seed)
+    print(json.dumps(line), flush=True)
+    pk.free()
+    ev.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+// grn_sim.h -- launch interface between the host evaluator and the
+// simulation kernels (grn_sim_kernel.cu).  Internal to the library.
+#ifndef GRN_SIM_H_
+#define GRN_SIM_H_
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "grn_packed.h"
+
+namespace grn {
+
+// Everything a simulation launch reads or writes.  Pointers are device
+// pointers.
+struct SimArgs {
+  const uint4 *packed;       // model records (grn_packed.h)
+  const int32_t *offsets;    // [n_models] first word of each record
+  int32_t n_models;
+  int32_t n_exp;             // experiments
+  int32_t n_in;              // input morphogens (initial channels)
+  int32_t n_target;          // target morphogens
+  int32_t W, H;              // grid width (x) and height (y)
+  int32_t Wg;                // float4 groups per row = ceil(W / 4)
+  int32_t n_steps;           // max Euler steps per experiment
+  int32_t fitness_kind;      // grn_fitness_kind
+  int32_t planes;            // state planes available per CTA
+  float dt;
+  float min_conc;
+  double min_conc_change;
+  double dist_threshold;
+  const float *initial;      // [n_exp][n_in][H][W]
+  const float *target;       // [n_exp][n_target][H][W]
+  const double *max_error;   // [caller index]
+  double *raw_error;         // [caller index] out
+  int32_t *steps;            // [caller index] out, may be null
+  int32_t *work_counter;     // zeroed before the launch
+  int32_t *error_flag;       // set non-zero on an internal error
+  float *gstate;             // global state slots (GLOBAL schedule)
+  int64_t slot_floats;       // floats per global state slot
+  float *state_out;          // optional final states
+                             // [caller index][n_exp][state_planes][H][W]
+  int32_t state_planes;
+};
+
+// One compiled kernel variant.
+struct KernelVariant {
+  int schedule;     // grn_schedule (SMEM_1BUF / SMEM_2BUF share a kernel)
+  int threads;      // threads per block
+  int gmax;         // most genes a model may have
+  int items;        // float4 groups per thread when genes sit in registers
+  int nreg;         // most genes whose new values wait in registers
+  bool global_state;
+};
+
+// Launch plan chosen by the host.
+struct LaunchPlan {
+  KernelVariant v;
+  int blocks;            // persistent grid size
+  int planes;            // state planes in shared memory (0 for GLOBAL)
+  size_t smem_bytes;     // dynamic shared memory
+  int blocks_per_sm;
+};
+
+// Bytes of shared memory a block needs besides the state planes.
+size_t sim_fixed_smem_bytes();
+
+// Number of compiled variants and their descriptions.
+int sim_variant_count();
+KernelVariant sim_variant(int i);
+
+// Occupancy of a variant with `smem_bytes` dynamic shared memory: resident
+// blocks per SM (0 if it does not fit).  Sets the function's max dynamic
+// shared memory attribute as a side effect.
+cudaError_t sim_occupancy(const KernelVariant &v, size_t smem_bytes,
+                          int *blocks_per_sm);
+
+// Launches a variant; the caller has zeroed args.work_counter on `stream`.
+cudaError_t sim_launch(const LaunchPlan &plan, const SimArgs &args,
+                       cudaStream_t stream);
+
+}  // namespace grn
+
+#endif  // GRN_SIM_H_

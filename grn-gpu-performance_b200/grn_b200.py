@@ -1,0 +1,342 @@
+"""Python binding of the B200 GRN evaluator (ctypes over libgrn_b200.so).
+
+The product is the C ABI in include/grn_gpu.h; this module is thin glue for
+tests, benchmarks and Python callers.  It loads the in-tree library and
+fails loudly if it is missing: there is no Python or CPU fallback.
+
+Models travel as numpy structured arrays whose layout is the C structs
+grn_product / grn_link.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgrn_b200.so")
+
+PRODUCT_DTYPE = np.dtype([("label", "<i4"), ("reserved0", "<i4"), ("init", "<f8"),
+                          ("lim", "<f8"), ("deg", "<f8"), ("dif", "<f8")])
+LINK_DTYPE = np.dtype([("regulator", "<i4"), ("regulated", "<i4"), ("dis_const", "<f8"),
+                       ("hill_coef", "<f8"), ("is_and", "<i4"), ("reserved0", "<i4")])
+assert PRODUCT_DTYPE.itemsize == 40 and LINK_DTYPE.itemsize == 32
+
+GRN_OK = 0
+STATUS_NAMES = {0: "GRN_OK", 1: "GRN_ERR_INVALID_ARGUMENT", 2: "GRN_ERR_NO_DEVICE",
+                3: "GRN_ERR_CUDA", 4: "GRN_ERR_OUT_OF_MEMORY", 5: "GRN_ERR_MODEL",
+                6: "GRN_ERR_CAPACITY", 7: "GRN_ERR_NO_EXPERIMENTS", 8: "GRN_ERR_TIMEOUT",
+                9: "GRN_ERR_NOT_FOUND", 10: "GRN_ERR_KERNEL"}
+FITNESS_REF_LOGTHRESH = 0
+FITNESS_MSE = 1
+SCHEDULE_AUTO, SCHEDULE_SMEM_1BUF, SCHEDULE_SMEM_2BUF, SCHEDULE_GLOBAL = 0, 1, 2, 3
+SCHEDULE_NAMES = {0: "auto", 1: "smem_regs", 2: "smem_2buf", 3: "global"}
+
+
+class SimParams(ctypes.Structure):
+    _fields_ = [("dim_x", ctypes.c_int32), ("dim_y", ctypes.c_int32),
+                ("n_input_morphogens", ctypes.c_int32), ("n_target_morphogens", ctypes.c_int32),
+                ("num_sim_steps", ctypes.c_int32), ("error_precision", ctypes.c_int32),
+                ("fitness_kind", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("dt", ctypes.c_double), ("min_conc", ctypes.c_double),
+                ("min_conc_change", ctypes.c_double), ("dist_error_threshold", ctypes.c_double)]
+
+    @classmethod
+    def from_dict(cls, d):
+        p = cls()
+        for name, _ in cls._fields_:
+            if name in d:
+                setattr(p, name, d[name])
+        return p
+
+
+class ModelBatchC(ctypes.Structure):
+    _fields_ = [("n_models", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("product_offsets", ctypes.c_void_p), ("products", ctypes.c_void_p),
+                ("link_offsets", ctypes.c_void_p), ("links", ctypes.c_void_p)]
+
+
+class EvalStats(ctypes.Structure):
+    _fields_ = [("n_models", ctypes.c_int64), ("cell_updates", ctypes.c_int64),
+                ("total_steps", ctypes.c_int64), ("kernel_ms", ctypes.c_double),
+                ("pack_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_int64),
+                ("d2h_bytes", ctypes.c_int64), ("schedule", ctypes.c_int32),
+                ("threads_per_block", ctypes.c_int32), ("blocks", ctypes.c_int32),
+                ("reserved0", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
+
+
+class PackedInfo(ctypes.Structure):
+    _fields_ = [("n_models", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("cell_update_bound", ctypes.c_int64), ("sfu_ops_per_step", ctypes.c_int64),
+                ("max_genes", ctypes.c_int32), ("max_links", ctypes.c_int32),
+                ("mean_genes", ctypes.c_double), ("mean_links", ctypes.c_double)]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_SIGNATURES = {
+    "grn_abi_version": ([], _I),
+    "grn_status_str": ([_I], ctypes.c_char_p),
+    "grn_last_error": ([_P], ctypes.c_char_p),
+    "grn_round_error": ([_D, _D, _I], _D),
+    "grn_create": ([ctypes.POINTER(_P), _I, ctypes.POINTER(SimParams)], _I),
+    "grn_destroy": ([_P], _I),
+    "grn_set_schedule": ([_P, _I, _I], _I),
+    "grn_set_experiments": ([_P, _I, _P, _P], _I),
+    "grn_set_experiments_rgb": ([_P, _I, _P, _P], _I),
+    "grn_decode_rgb": ([_I, _I, _I, _P, _P], _I),
+    "grn_evaluate": ([_P, _P, _I, _P, _I, _D, ctypes.POINTER(_D)], _I),
+    "grn_evaluate_batch": ([_P, ctypes.POINTER(ModelBatchC), _P, _P, _P,
+                            ctypes.POINTER(EvalStats)], _I),
+    "grn_evaluate_states": ([_P, ctypes.POINTER(ModelBatchC), _P, _P, _P, _I], _I),
+    "grn_submit": ([_P, _I, ctypes.POINTER(ModelBatchC), _P, _P, _P], _I),
+    "grn_wait_any": ([_P, _I, ctypes.POINTER(_I)], _I),
+    "grn_pack": ([_P, ctypes.POINTER(ModelBatchC), ctypes.POINTER(_P)], _I),
+    "grn_packed_free": ([_P], _I),
+    "grn_packed_get_info": ([_P, ctypes.POINTER(PackedInfo)], _I),
+    "grn_run_packed": ([_P, _P, _P, _P, _P, _P], _I),
+    "grn_describe_model": ([_P, _I, _P, _I, _I, ctypes.c_char_p, _I], _I),
+}
+
+_lib = None
+
+
+class GrnError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("%s%s" % (STATUS_NAMES.get(status, str(status)), (": " + msg) if msg else ""))
+
+
+def load_library(path=LIB_PATH):
+    """Loads libgrn_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libgrn_b200.so not built: run `python grn-gpu-performance_b200/build.py`"
+                           " (there is no fallback path)")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class ModelBatch:
+    """Models in genome form (the C struct grn_model_batch)."""
+
+    def __init__(self, product_offsets, products, link_offsets, links):
+        self.product_offsets = np.ascontiguousarray(product_offsets, dtype=np.int32)
+        self.products = np.ascontiguousarray(products, dtype=PRODUCT_DTYPE)
+        self.link_offsets = np.ascontiguousarray(link_offsets, dtype=np.int32)
+        self.links = np.ascontiguousarray(links, dtype=LINK_DTYPE)
+        assert len(self.product_offsets) == len(self.link_offsets)
+
+    @property
+    def n_models(self):
+        return len(self.product_offsets) - 1
+
+    @classmethod
+    def from_models(cls, models):
+        """models: list of (products array, links array)."""
+        po, lo = [0], [0]
+        for p, l in models:
+            po.append(po[-1] + len(p))
+            lo.append(lo[-1] + len(l))
+        prods = np.concatenate([np.asarray(p, PRODUCT_DTYPE) for p, _ in models]) if models else \
+            np.zeros(0, PRODUCT_DTYPE)
+        links = np.concatenate([np.asarray(l, LINK_DTYPE) for _, l in models]) if models else \
+            np.zeros(0, LINK_DTYPE)
+        return cls(po, prods, lo, links)
+
+    def model(self, i):
+        return (self.products[self.product_offsets[i]:self.product_offsets[i + 1]],
+                self.links[self.link_offsets[i]:self.link_offsets[i + 1]])
+
+    def subset(self, idx):
+        return ModelBatch.from_models([self.model(int(i)) for i in idx])
+
+    def as_c(self):
+        c = ModelBatchC()
+        c.n_models = self.n_models
+        c.product_offsets = _ptr(self.product_offsets)
+        c.products = _ptr(self.products) if len(self.products) else None
+        c.link_offsets = _ptr(self.link_offsets)
+        c.links = _ptr(self.links) if len(self.links) else None
+        return c
+
+
+def round_error(raw, max_error, precision):
+    return load_library().grn_round_error(float(raw), float(max_error), int(precision))
+
+
+def decode_rgb(pixels, n_channels):
+    """0xAARRGGBB pixels [H][W] -> planar channels [n][H][W] (reference y flip)."""
+    lib = load_library()
+    px = np.ascontiguousarray(pixels, dtype=np.uint32)
+    h, w = px.shape
+    out = np.zeros((n_channels, h, w), np.float64)
+    _check(lib.grn_decode_rgb(w, h, n_channels, _ptr(px), _ptr(out)))
+    return out
+
+
+def describe_model(products, links, n_morphogens):
+    """Text listing of the compiled program of one model (see grn_gpu.h)."""
+    lib = load_library()
+    p = np.ascontiguousarray(products, PRODUCT_DTYPE)
+    l = np.ascontiguousarray(links, LINK_DTYPE)
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(lib.grn_describe_model(_ptr(p), len(p), _ptr(l) if len(l) else None, len(l),
+                                  n_morphogens, buf, len(buf)))
+    return buf.value.decode()
+
+
+def _check(status, ctx=None):
+    if status != GRN_OK:
+        msg = ""
+        if ctx:
+            msg = load_library().grn_last_error(ctx).decode()
+        raise GrnError(status, msg)
+
+
+class Evaluator:
+    """One grn_ctx: a device, a stream, the uploaded experiments."""
+
+    def __init__(self, params, device=0):
+        self.lib = load_library()
+        self.params = dict(params)
+        self._p = SimParams.from_dict(self.params)
+        ctx = ctypes.c_void_p()
+        _check(self.lib.grn_create(ctypes.byref(ctx), device, ctypes.byref(self._p)))
+        self.ctx = ctx
+        self._keep = {}
+
+    def close(self):
+        if self.ctx:
+            self.lib.grn_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_schedule(self, schedule, threads=0):
+        _check(self.lib.grn_set_schedule(self.ctx, schedule, threads), self.ctx)
+
+    def set_experiments(self, initial, target):
+        """initial [n_exp][n_in][H][W], target [n_exp][n_target][H][W] (float64)."""
+        ini = np.ascontiguousarray(initial, np.float64)
+        tgt = np.ascontiguousarray(target, np.float64)
+        _check(self.lib.grn_set_experiments(self.ctx, ini.shape[0], _ptr(ini), _ptr(tgt)), self.ctx)
+        self._n_exp = ini.shape[0]
+
+    def set_experiments_rgb(self, input_pixels, target_pixels):
+        a = np.ascontiguousarray(input_pixels, np.uint32)
+        b = np.ascontiguousarray(target_pixels, np.uint32)
+        _check(self.lib.grn_set_experiments_rgb(self.ctx, a.shape[0], _ptr(a), _ptr(b)), self.ctx)
+        self._n_exp = a.shape[0]
+
+    def evaluate(self, products, links, max_error=1000.0):
+        p = np.ascontiguousarray(products, PRODUCT_DTYPE)
+        l = np.ascontiguousarray(links, LINK_DTYPE)
+        out = ctypes.c_double()
+        _check(self.lib.grn_evaluate(self.ctx, _ptr(p), len(p), _ptr(l) if len(l) else None,
+                                     len(l), float(max_error), ctypes.byref(out)), self.ctx)
+        return out.value
+
+    def evaluate_batch(self, batch, max_error=None):
+        """Returns (rounded errors, raw errors, stats dict)."""
+        n = batch.n_models
+        me = np.full(n, 1000.0) if max_error is None else \
+            np.ascontiguousarray(np.broadcast_to(np.asarray(max_error, np.float64), (n,)))
+        err = np.zeros(n, np.float64)
+        raw = np.zeros(n, np.float64)
+        st = EvalStats()
+        cb = batch.as_c()
+        _check(self.lib.grn_evaluate_batch(self.ctx, ctypes.byref(cb), _ptr(me), _ptr(err),
+                                           _ptr(raw), ctypes.byref(st)), self.ctx)
+        return err, raw, st.as_dict()
+
+    def evaluate_states(self, batch, max_error=None, max_planes=16):
+        """Returns (raw errors, final states [n][n_exp][max_planes][H][W] float32)."""
+        n = batch.n_models
+        me = np.full(n, 1000.0) if max_error is None else \
+            np.ascontiguousarray(np.broadcast_to(np.asarray(max_error, np.float64), (n,)))
+        raw = np.zeros(n, np.float64)
+        n_exp = self._n_exp
+        st = np.zeros((n, n_exp, max_planes, self.params["dim_y"], self.params["dim_x"]),
+                      np.float32)
+        cb = batch.as_c()
+        _check(self.lib.grn_evaluate_states(self.ctx, ctypes.byref(cb), _ptr(me), _ptr(raw),
+                                            _ptr(st), max_planes), self.ctx)
+        return raw, st
+
+    def submit(self, tag, batch, max_error=None):
+        n = batch.n_models
+        me = np.full(n, 1000.0) if max_error is None else \
+            np.ascontiguousarray(np.broadcast_to(np.asarray(max_error, np.float64), (n,)))
+        err = np.zeros(n, np.float64)
+        raw = np.zeros(n, np.float64)
+        cb = batch.as_c()
+        _check(self.lib.grn_submit(self.ctx, int(tag), ctypes.byref(cb), _ptr(me), _ptr(err),
+                                   _ptr(raw)), self.ctx)
+        self._keep[int(tag)] = (err, raw, me, batch)
+        return err, raw
+
+    def wait_any(self, timeout_ms=-1):
+        tag = ctypes.c_int()
+        _check(self.lib.grn_wait_any(self.ctx, int(timeout_ms), ctypes.byref(tag)), self.ctx)
+        err, raw, _, _ = self._keep.pop(tag.value)
+        return tag.value, err, raw
+
+    def pack(self, batch):
+        return Packed(self, batch)
+
+
+class Packed:
+    """A batch compiled and resident on the device (grn_pack)."""
+
+    def __init__(self, ev, batch):
+        self.ev = ev
+        h = ctypes.c_void_p()
+        cb = batch.as_c()
+        _check(ev.lib.grn_pack(ev.ctx, ctypes.byref(cb), ctypes.byref(h)), ev.ctx)
+        self.handle = h
+        info = PackedInfo()
+        _check(ev.lib.grn_packed_get_info(h, ctypes.byref(info)))
+        self.info = {name: getattr(info, name) for name, _ in PackedInfo._fields_}
+
+    def run(self, d_max_error, d_raw_error, d_steps=None, stream=None):
+        """Device pointers (ints); stream is a cudaStream_t as int or None."""
+        _check(self.ev.lib.grn_run_packed(self.ev.ctx, self.handle, ctypes.c_void_p(d_max_error),
+                                          ctypes.c_void_p(d_raw_error),
+                                          ctypes.c_void_p(d_steps) if d_steps else None,
+                                          ctypes.c_void_p(stream) if stream else None), self.ev.ctx)
+
+    def free(self):
+        if self.handle:
+            self.ev.lib.grn_packed_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

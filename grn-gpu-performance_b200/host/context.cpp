@@ -1,0 +1,806 @@
+// context.cpp -- the C ABI of include/grn_gpu.h.
+//
+// Host side of the evaluator: the B200 counterpart of the reference's
+// CEvaluatorMorphogens + CModelSimulator (Src/GPUSimulator/*.cpp).  One
+// context = one device + one stream; experiments are uploaded once; a batch
+// is compiled on the host (pack.cpp), copied from pinned staging buffers,
+// simulated by one persistent kernel launch and read back as raw errors,
+// which are rounded here exactly as the reference's evaluate does.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/grn_gpu.h"
+#include "../csrc/grn_sim.h"
+#include "pack.h"
+
+namespace {
+
+using grn::LaunchPlan;
+using grn::PackedHost;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+struct HostBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+// Scratch of one in-flight evaluation: device buffers, pinned staging and a
+// completion event.
+struct Job {
+  DevBuf d_words, d_offsets, d_maxerr, d_raw, d_steps, d_flag;
+  HostBuf h_words, h_offsets, h_maxerr, h_raw, h_steps, h_flag;
+  cudaEvent_t ev_start = nullptr, ev_kernel = nullptr, ev_done = nullptr;
+  // Results of an asynchronous submission.
+  int tag = 0;
+  int n_models = 0;
+  double *error_out = nullptr;
+  double *raw_out = nullptr;
+  std::vector<double> max_error;
+  int64_t cells = 0;
+};
+
+}  // namespace
+
+struct grn_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  grn_sim_params p{};
+  std::string last_error;
+  int n_sm = 0;
+  int smem_optin = 0;
+  int n_exp = 0;
+  DevBuf d_initial, d_target, d_counter, d_gstate;
+  Job sync_job;
+  std::deque<Job *> pending;
+  std::vector<Job *> free_jobs;
+  int forced_schedule = GRN_SCHEDULE_AUTO;
+  int forced_threads = 0;
+};
+
+struct grn_packed {
+  grn_ctx *ctx = nullptr;
+  PackedHost host;
+  DevBuf d_words, d_offsets;
+  int64_t cell_bound = 0;
+};
+
+namespace {
+
+grn_status fail(grn_ctx *ctx, grn_status s, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+  return s;
+}
+
+grn_status cuda_fail(grn_ctx *ctx, cudaError_t e, const char *what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  return fail(ctx, e == cudaErrorMemoryAllocation ? GRN_ERR_OUT_OF_MEMORY : GRN_ERR_CUDA, msg);
+}
+
+#define GRN_CUDA(ctx, expr)                               \
+  do {                                                    \
+    cudaError_t e__ = (expr);                             \
+    if (e__ != cudaSuccess) return cuda_fail(ctx, e__, #expr); \
+  } while (0)
+
+grn_status ensure_dev(grn_ctx *ctx, DevBuf *b, size_t bytes) {
+  if (bytes <= b->cap) return GRN_OK;
+  if (b->p) cudaFree(b->p);
+  b->p = nullptr;
+  b->cap = 0;
+  size_t cap = std::max<size_t>(bytes + bytes / 4, 256);
+  GRN_CUDA(ctx, cudaMalloc(&b->p, cap));
+  b->cap = cap;
+  return GRN_OK;
+}
+
+grn_status ensure_host(grn_ctx *ctx, HostBuf *b, size_t bytes) {
+  if (bytes <= b->cap) return GRN_OK;
+  if (b->p) cudaFreeHost(b->p);
+  b->p = nullptr;
+  b->cap = 0;
+  size_t cap = std::max<size_t>(bytes + bytes / 4, 256);
+  GRN_CUDA(ctx, cudaHostAlloc(&b->p, cap, cudaHostAllocDefault));
+  b->cap = cap;
+  return GRN_OK;
+}
+
+void free_job(Job *j) {
+  for (DevBuf *b : {&j->d_words, &j->d_offsets, &j->d_maxerr, &j->d_raw, &j->d_steps, &j->d_flag})
+    if (b->p) cudaFree(b->p);
+  for (HostBuf *b : {&j->h_words, &j->h_offsets, &j->h_maxerr, &j->h_raw, &j->h_steps, &j->h_flag})
+    if (b->p) cudaFreeHost(b->p);
+  for (cudaEvent_t e : {j->ev_start, j->ev_kernel, j->ev_done})
+    if (e) cudaEventDestroy(e);
+}
+
+grn_status check_params(const grn_sim_params *p) {
+  if (!p) return GRN_ERR_INVALID_ARGUMENT;
+  if (p->dim_x < 1 || p->dim_y < 1 || p->dim_x > 4096 || p->dim_y > 4096)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (p->n_input_morphogens < 0 || p->n_input_morphogens > GRN_MAX_INPUT_MORPHOGENS)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (p->n_target_morphogens < 0 || p->n_target_morphogens > 3)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (p->n_input_morphogens + p->n_target_morphogens > GRN_MAX_GENES)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (p->num_sim_steps < 0 || p->error_precision < 0 || p->error_precision > 17)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (p->fitness_kind != GRN_FITNESS_REF_LOGTHRESH && p->fitness_kind != GRN_FITNESS_MSE)
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(p->dt)) return GRN_ERR_INVALID_ARGUMENT;
+  return GRN_OK;
+}
+
+grn_status check_batch(grn_ctx *ctx, const grn_model_batch *b) {
+  if (!b || b->n_models < 0) return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null batch");
+  if (b->n_models == 0) return GRN_OK;
+  if (!b->product_offsets || !b->link_offsets)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null offsets");
+  if (b->product_offsets[0] != 0 || b->link_offsets[0] != 0)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "offsets must start at 0");
+  for (int m = 0; m < b->n_models; ++m) {
+    if (b->product_offsets[m + 1] < b->product_offsets[m] ||
+        b->link_offsets[m + 1] < b->link_offsets[m])
+      return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "offsets must not decrease");
+  }
+  if (b->product_offsets[b->n_models] > 0 && !b->products)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null products");
+  if (b->link_offsets[b->n_models] > 0 && !b->links)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null links");
+  return GRN_OK;
+}
+
+int host_threads() {
+  unsigned n = std::thread::hardware_concurrency();
+  return n ? (int)n : 1;
+}
+
+// Autotuner, first stage: every compiled kernel variant that can hold the
+// batch is scored by its resident useful threads per SM (occupancy x
+// threads that own a group); layouts that double-buffer every gene (one
+// barrier per step) are preferred over ones that hold some genes' new values
+// in registers (two barriers per step).
+grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *out) {
+  const int W = ctx->p.dim_x, H = ctx->p.dim_y;
+  const int Wg = (W + 3) / 4, Q = H * Wg;
+  const size_t plane_bytes = (size_t)H * Wg * 4 * sizeof(float);
+  const size_t fixed = grn::sim_fixed_smem_bytes();
+  const size_t optin = (size_t)ctx->smem_optin;
+  const int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) : 0;
+  double best_score = -1;
+  LaunchPlan best{};
+  const int nv = grn::sim_variant_count();
+  if (ctx->forced_schedule != GRN_SCHEDULE_GLOBAL) {
+    for (int i = 0; i < nv; ++i) {
+      grn::KernelVariant v = grn::sim_variant(i);
+      if (v.global_state || v.gmax < max_genes) continue;
+      if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
+      // Candidate plane counts: as many as useful, or the fewest this
+      // variant can run with (more blocks per SM).
+      const int cands[2] = {std::min(fit, 2 * max_genes),
+                            std::max(max_genes, 2 * max_genes - v.nreg)};
+      for (int planes : cands) {
+        if (planes < max_genes || planes > fit) continue;
+        const int n_reg = std::max(0, 2 * max_genes - planes);
+        if (n_reg > v.nreg) continue;
+        if (n_reg > 0 && Q > v.threads * v.items) continue;
+        if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_2BUF && n_reg > 0) continue;
+        if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_1BUF && n_reg == 0) continue;
+        const size_t smem = fixed + planes * plane_bytes;
+        int occ = 0;
+        GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &occ));
+        if (occ < 1) continue;
+        double score = (double)occ * std::min(v.threads, Q) * (n_reg == 0 ? 1.25 : 1.0);
+        score -= 1e-3 * (v.gmax + v.nreg);  // prefer the tighter register footprint
+        if (score > best_score) {
+          best_score = score;
+          best.v = v;
+          best.v.schedule = n_reg == 0 ? GRN_SCHEDULE_SMEM_2BUF : GRN_SCHEDULE_SMEM_1BUF;
+          best.planes = planes;
+          best.smem_bytes = smem;
+          best.blocks_per_sm = occ;
+        }
+      }
+    }
+  }
+  if (best_score < 0) {
+    if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_1BUF ||
+        ctx->forced_schedule == GRN_SCHEDULE_SMEM_2BUF)
+      return fail(ctx, GRN_ERR_CAPACITY, "forced shared-memory schedule cannot hold the grid");
+    // Global-memory state slots.
+    for (int i = 0; i < nv; ++i) {
+      grn::KernelVariant v = grn::sim_variant(i);
+      if (!v.global_state || v.gmax < max_genes) continue;
+      if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
+      int occ = 0;
+      GRN_CUDA(ctx, grn::sim_occupancy(v, fixed, &occ));
+      if (occ < 1) continue;
+      double score = (double)occ * v.threads - 1e-3 * v.gmax;
+      if (score > best_score) {
+        best_score = score;
+        best.v = v;
+        best.planes = 0;
+        best.smem_bytes = fixed;
+        best.blocks_per_sm = occ;
+      }
+    }
+  }
+  if (best_score < 0)
+    return fail(ctx, GRN_ERR_CAPACITY, "no kernel variant holds " +
+                                           std::to_string(max_genes) + " genes");
+  best.blocks = std::max(1, std::min(n_models, ctx->n_sm * best.blocks_per_sm));
+  *out = best;
+  return GRN_OK;
+}
+
+// Launches the simulation of `n_models` packed records already on the
+// device.  `stream` may differ from the context's stream.
+grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
+                         int n_models, int max_genes, const double *d_max_error,
+                         double *d_raw, int32_t *d_steps, int32_t *d_flag,
+                         cudaStream_t stream, LaunchPlan *plan_out,
+                         float *d_states = nullptr, int state_planes = 0) {
+  if (n_models == 0) return GRN_OK;
+  if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
+  LaunchPlan plan;
+  grn_status s = choose_plan(ctx, max_genes, n_models, &plan);
+  if (s != GRN_OK) return s;
+  const int W = ctx->p.dim_x, H = ctx->p.dim_y, Wg = (W + 3) / 4;
+  grn::SimArgs a{};
+  a.packed = d_words;
+  a.offsets = d_offsets;
+  a.n_models = n_models;
+  a.n_exp = ctx->n_exp;
+  a.n_in = ctx->p.n_input_morphogens;
+  a.n_target = ctx->p.n_target_morphogens;
+  a.W = W;
+  a.H = H;
+  a.Wg = Wg;
+  a.n_steps = ctx->p.num_sim_steps;
+  a.fitness_kind = ctx->p.fitness_kind;
+  a.planes = plan.planes;
+  a.dt = (float)ctx->p.dt;
+  a.min_conc = (float)ctx->p.min_conc;
+  a.min_conc_change = ctx->p.min_conc_change;
+  a.dist_threshold = ctx->p.dist_error_threshold;
+  a.initial = static_cast<const float *>(ctx->d_initial.p);
+  a.target = static_cast<const float *>(ctx->d_target.p);
+  a.max_error = d_max_error;
+  a.raw_error = d_raw;
+  a.steps = d_steps;
+  a.work_counter = static_cast<int32_t *>(ctx->d_counter.p);
+  a.error_flag = d_flag;
+  a.state_out = d_states;
+  a.state_planes = state_planes;
+  if (plan.v.global_state) {
+    const int64_t slot = 2LL * plan.v.gmax * H * Wg * 4;
+    s = ensure_dev(ctx, &ctx->d_gstate, (size_t)slot * plan.blocks * sizeof(float));
+    if (s != GRN_OK) return s;
+    a.gstate = static_cast<float *>(ctx->d_gstate.p);
+    a.slot_floats = slot;
+  }
+  GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int32_t), stream));
+  GRN_CUDA(ctx, grn::sim_launch(plan, a, stream));
+  if (plan_out) *plan_out = plan;
+  return GRN_OK;
+}
+
+// Compiles a batch and enqueues copy-in, kernel and copy-out on the
+// context's stream into job `j`.
+grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
+                       const double *max_error, grn_eval_stats *stats) {
+  grn_status s = check_batch(ctx, batch);
+  if (s != GRN_OK) return s;
+  if (!max_error) return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null max_error");
+  if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
+  const int n = batch->n_models;
+  j->n_models = n;
+  auto t0 = std::chrono::steady_clock::now();
+  PackedHost ph;
+  std::string err;
+  s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      host_threads(), &ph, &err);
+  if (s != GRN_OK) return fail(ctx, s, err);
+  auto t1 = std::chrono::steady_clock::now();
+  if (n == 0) return GRN_OK;
+  const size_t wb = ph.words.size() * sizeof(uint4), ob = n * sizeof(int32_t);
+  const size_t eb = n * sizeof(double), sb = n * sizeof(int32_t);
+  if ((s = ensure_dev(ctx, &j->d_words, wb)) || (s = ensure_dev(ctx, &j->d_offsets, ob)) ||
+      (s = ensure_dev(ctx, &j->d_maxerr, eb)) || (s = ensure_dev(ctx, &j->d_raw, eb)) ||
+      (s = ensure_dev(ctx, &j->d_steps, sb)) || (s = ensure_dev(ctx, &j->d_flag, 4)) ||
+      (s = ensure_host(ctx, &j->h_words, wb)) || (s = ensure_host(ctx, &j->h_offsets, ob)) ||
+      (s = ensure_host(ctx, &j->h_maxerr, eb)) || (s = ensure_host(ctx, &j->h_raw, eb)) ||
+      (s = ensure_host(ctx, &j->h_steps, sb)) || (s = ensure_host(ctx, &j->h_flag, 4)))
+    return s;
+  if (!j->ev_start) {
+    GRN_CUDA(ctx, cudaEventCreate(&j->ev_start));
+    GRN_CUDA(ctx, cudaEventCreate(&j->ev_kernel));
+    GRN_CUDA(ctx, cudaEventCreate(&j->ev_done));
+  }
+  std::memcpy(j->h_words.p, ph.words.data(), wb);
+  std::memcpy(j->h_offsets.p, ph.offsets.data(), ob);
+  std::memcpy(j->h_maxerr.p, max_error, eb);
+  cudaStream_t st = ctx->stream;
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->d_words.p, j->h_words.p, wb, cudaMemcpyHostToDevice, st));
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->d_offsets.p, j->h_offsets.p, ob, cudaMemcpyHostToDevice, st));
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->d_maxerr.p, j->h_maxerr.p, eb, cudaMemcpyHostToDevice, st));
+  GRN_CUDA(ctx, cudaMemsetAsync(j->d_flag.p, 0, 4, st));
+  GRN_CUDA(ctx, cudaEventRecord(j->ev_start, st));
+  LaunchPlan plan{};
+  s = launch_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
+                    static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes,
+                    static_cast<const double *>(j->d_maxerr.p),
+                    static_cast<double *>(j->d_raw.p), static_cast<int32_t *>(j->d_steps.p),
+                    static_cast<int32_t *>(j->d_flag.p), st, &plan);
+  if (s != GRN_OK) return s;
+  GRN_CUDA(ctx, cudaEventRecord(j->ev_kernel, st));
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->h_raw.p, j->d_raw.p, eb, cudaMemcpyDeviceToHost, st));
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->h_steps.p, j->d_steps.p, sb, cudaMemcpyDeviceToHost, st));
+  GRN_CUDA(ctx, cudaMemcpyAsync(j->h_flag.p, j->d_flag.p, 4, cudaMemcpyDeviceToHost, st));
+  GRN_CUDA(ctx, cudaEventRecord(j->ev_done, st));
+  j->cells = (int64_t)ctx->p.dim_x * ctx->p.dim_y;
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->n_models = n;
+    stats->pack_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    stats->h2d_bytes = (int64_t)(wb + ob + eb);
+    stats->d2h_bytes = (int64_t)(eb + sb + 4);
+    stats->schedule = plan.v.schedule;
+    stats->threads_per_block = plan.v.threads;
+    stats->blocks = plan.blocks;
+  }
+  return GRN_OK;
+}
+
+// Reads back a finished job: rounding as CEvaluatorMorphogens::evaluate
+// (cevaluatormorphogens.cpp:233-245).
+grn_status finish_job(grn_ctx *ctx, Job *j, const double *max_error, double *error_out,
+                      double *raw_out, grn_eval_stats *stats) {
+  const int n = j->n_models;
+  if (n == 0) return GRN_OK;
+  if (*static_cast<int32_t *>(j->h_flag.p) != 0)
+    return fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected a model record");
+  const double *raw = static_cast<const double *>(j->h_raw.p);
+  const int32_t *steps = static_cast<const int32_t *>(j->h_steps.p);
+  int64_t total_steps = 0;
+  for (int m = 0; m < n; ++m) {
+    if (error_out) error_out[m] = grn_round_error(raw[m], max_error[m], ctx->p.error_precision);
+    if (raw_out) raw_out[m] = raw[m];
+    total_steps += steps[m];
+  }
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, j->ev_start, j->ev_kernel);
+    stats->kernel_ms = ms;
+    stats->total_steps = total_steps;
+    stats->cell_updates = total_steps * j->cells;
+  }
+  return GRN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grn_abi_version(void) { return GRN_ABI_VERSION; }
+
+const char *grn_status_str(grn_status s) {
+  switch (s) {
+    case GRN_OK: return "GRN_OK";
+    case GRN_ERR_INVALID_ARGUMENT: return "GRN_ERR_INVALID_ARGUMENT";
+    case GRN_ERR_NO_DEVICE: return "GRN_ERR_NO_DEVICE";
+    case GRN_ERR_CUDA: return "GRN_ERR_CUDA";
+    case GRN_ERR_OUT_OF_MEMORY: return "GRN_ERR_OUT_OF_MEMORY";
+    case GRN_ERR_MODEL: return "GRN_ERR_MODEL";
+    case GRN_ERR_CAPACITY: return "GRN_ERR_CAPACITY";
+    case GRN_ERR_NO_EXPERIMENTS: return "GRN_ERR_NO_EXPERIMENTS";
+    case GRN_ERR_TIMEOUT: return "GRN_ERR_TIMEOUT";
+    case GRN_ERR_NOT_FOUND: return "GRN_ERR_NOT_FOUND";
+    case GRN_ERR_KERNEL: return "GRN_ERR_KERNEL";
+  }
+  return "GRN_ERR_UNKNOWN";
+}
+
+const char *grn_last_error(const grn_ctx *ctx) {
+  return ctx ? ctx->last_error.c_str() : "";
+}
+
+double grn_round_error(double raw, double max_error, int precision) {
+  // CEvaluatorMorphogens::evaluate + MathAlgo::ceilS (Src/Common/mathalgo.h:55-62).
+  if (raw > max_error) return 100;
+  if (raw == 0.0) return 0.0;
+  const double factor = std::pow(10.0, precision - std::ceil(std::log10(std::fabs(raw))));
+  return std::ceil(raw * factor) / factor;
+}
+
+grn_status grn_create(grn_ctx **out, int device, const grn_sim_params *params) {
+  if (!out) return GRN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  grn_status s = check_params(params);
+  if (s != GRN_OK) return s;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev < 1) {
+    cudaGetLastError();
+    return GRN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n_dev) return GRN_ERR_NO_DEVICE;
+  grn_ctx *ctx = new (std::nothrow) grn_ctx();
+  if (!ctx) return GRN_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  ctx->p = *params;
+  auto bail = [&](grn_status st) {
+    grn_destroy(ctx);
+    return st;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(GRN_ERR_NO_DEVICE);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(GRN_ERR_CUDA);
+  cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (ensure_dev(ctx, &ctx->d_counter, 16) != GRN_OK) return bail(GRN_ERR_OUT_OF_MEMORY);
+  *out = ctx;
+  return GRN_OK;
+}
+
+grn_status grn_destroy(grn_ctx *ctx) {
+  if (!ctx) return GRN_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (Job *j : ctx->pending) {
+    free_job(j);
+    delete j;
+  }
+  for (Job *j : ctx->free_jobs) {
+    free_job(j);
+    delete j;
+  }
+  free_job(&ctx->sync_job);
+  for (DevBuf *b : {&ctx->d_initial, &ctx->d_target, &ctx->d_counter, &ctx->d_gstate})
+    if (b->p) cudaFree(b->p);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return GRN_OK;
+}
+
+grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_GLOBAL || threads_per_block < 0)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad schedule");
+  ctx->forced_schedule = schedule;
+  ctx->forced_threads = threads_per_block;
+  return GRN_OK;
+}
+
+grn_status grn_set_experiments(grn_ctx *ctx, int n_experiments, const double *initial,
+                               const double *target) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (n_experiments < 1 || n_experiments > GRN_MAX_EXPERIMENTS || !initial || !target)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad experiments");
+  cudaSetDevice(ctx->device);
+  const size_t plane = (size_t)ctx->p.dim_x * ctx->p.dim_y;
+  const size_t ni = n_experiments * ctx->p.n_input_morphogens * plane;
+  const size_t nt = n_experiments * ctx->p.n_target_morphogens * plane;
+  std::vector<float> fi(ni), ft(nt);
+  for (size_t i = 0; i < ni; ++i) fi[i] = (float)initial[i];
+  for (size_t i = 0; i < nt; ++i) ft[i] = (float)target[i];
+  grn_status s;
+  if ((s = ensure_dev(ctx, &ctx->d_initial, std::max<size_t>(ni, 1) * sizeof(float))) ||
+      (s = ensure_dev(ctx, &ctx->d_target, std::max<size_t>(nt, 1) * sizeof(float))))
+    return s;
+  if (ni) GRN_CUDA(ctx, cudaMemcpyAsync(ctx->d_initial.p, fi.data(), ni * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  if (nt) GRN_CUDA(ctx, cudaMemcpyAsync(ctx->d_target.p, ft.data(), nt * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  GRN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->n_exp = n_experiments;
+  return GRN_OK;
+}
+
+grn_status grn_decode_rgb(int dim_x, int dim_y, int n_channels, const uint32_t *pixels,
+                          double *out) {
+  if (dim_x < 1 || dim_y < 1 || n_channels < 0 || n_channels > 3 || !pixels || !out)
+    return GRN_ERR_INVALID_ARGUMENT;
+  // SimState::loadMorphologyImage (Src/Simulator/simstate.cpp:71-90):
+  // scanline j fills row H-1-j; channel k is byte (16 - 8k) of 0xAARRGGBB.
+  const size_t plane = (size_t)dim_x * dim_y;
+  for (int j = 0; j < dim_y; ++j)
+    for (int i = 0; i < dim_x; ++i) {
+      const uint32_t color = pixels[(size_t)j * dim_x + i];
+      for (int k = 0; k < n_channels; ++k)
+        out[k * plane + (size_t)(dim_y - j - 1) * dim_x + i] =
+            (double)((color >> (16 - 8 * k)) & 0xffu) / 255.0;
+    }
+  return GRN_OK;
+}
+
+grn_status grn_set_experiments_rgb(grn_ctx *ctx, int n_experiments, const uint32_t *input_pixels,
+                                   const uint32_t *target_pixels) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (n_experiments < 1 || n_experiments > GRN_MAX_EXPERIMENTS || !input_pixels || !target_pixels)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad experiments");
+  const int W = ctx->p.dim_x, H = ctx->p.dim_y;
+  const int ni = ctx->p.n_input_morphogens, nt = ctx->p.n_target_morphogens;
+  const size_t plane = (size_t)W * H;
+  std::vector<double> init((size_t)n_experiments * ni * plane), tgt((size_t)n_experiments * nt * plane);
+  for (int e = 0; e < n_experiments; ++e) {
+    grn_decode_rgb(W, H, ni, input_pixels + e * plane, init.data() + e * ni * plane);
+    grn_decode_rgb(W, H, nt, target_pixels + e * plane, tgt.data() + e * nt * plane);
+  }
+  return grn_set_experiments(ctx, n_experiments, init.data(), tgt.data());
+}
+
+grn_status grn_evaluate_batch(grn_ctx *ctx, const grn_model_batch *batch, const double *max_error,
+                              double *error_out, double *raw_error_out, grn_eval_stats *stats) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (!error_out && !raw_error_out)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "no output buffer");
+  cudaSetDevice(ctx->device);
+  grn_status s = enqueue_job(ctx, &ctx->sync_job, batch, max_error, stats);
+  if (s != GRN_OK) return s;
+  if (batch->n_models == 0) return GRN_OK;
+  GRN_CUDA(ctx, cudaEventSynchronize(ctx->sync_job.ev_done));
+  return finish_job(ctx, &ctx->sync_job, max_error, error_out, raw_error_out, stats);
+}
+
+grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const double *max_error,
+                               double *raw_error_out, float *states_out, int max_planes) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  grn_status s = check_batch(ctx, batch);
+  if (s != GRN_OK) return s;
+  if (!max_error || !states_out || max_planes < 1)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad states request");
+  if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
+  const int n = batch->n_models;
+  if (n == 0) return GRN_OK;
+  cudaSetDevice(ctx->device);
+  PackedHost ph;
+  std::string err;
+  s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      host_threads(), &ph, &err);
+  if (s != GRN_OK) return fail(ctx, s, err);
+  Job &j = ctx->sync_job;
+  const size_t wb = ph.words.size() * sizeof(uint4), ob = n * sizeof(int32_t);
+  const size_t eb = n * sizeof(double);
+  const size_t sb = (size_t)n * ctx->n_exp * max_planes * ctx->p.dim_x * ctx->p.dim_y * sizeof(float);
+  DevBuf d_states;
+  if ((s = ensure_dev(ctx, &j.d_words, wb)) || (s = ensure_dev(ctx, &j.d_offsets, ob)) ||
+      (s = ensure_dev(ctx, &j.d_maxerr, eb)) || (s = ensure_dev(ctx, &j.d_raw, eb)) ||
+      (s = ensure_dev(ctx, &j.d_steps, ob)) || (s = ensure_dev(ctx, &j.d_flag, 4)) ||
+      (s = ensure_dev(ctx, &d_states, sb)))
+    return s;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(cudaMemcpyAsync(j.d_words.p, ph.words.data(), wb, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j.d_offsets.p, ph.offsets.data(), ob, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j.d_maxerr.p, max_error, eb, cudaMemcpyHostToDevice, st));
+  chk(cudaMemsetAsync(j.d_flag.p, 0, 4, st));
+  chk(cudaMemsetAsync(d_states.p, 0, sb, st));
+  if (e == cudaSuccess) {
+    s = launch_packed(ctx, static_cast<const uint4 *>(j.d_words.p),
+                      static_cast<const int32_t *>(j.d_offsets.p), n, ph.max_genes,
+                      static_cast<const double *>(j.d_maxerr.p), static_cast<double *>(j.d_raw.p),
+                      static_cast<int32_t *>(j.d_steps.p), static_cast<int32_t *>(j.d_flag.p), st,
+                      nullptr, static_cast<float *>(d_states.p), max_planes);
+    int32_t flag = 0;
+    chk(cudaMemcpyAsync(states_out, d_states.p, sb, cudaMemcpyDeviceToHost, st));
+    if (raw_error_out) chk(cudaMemcpyAsync(raw_error_out, j.d_raw.p, eb, cudaMemcpyDeviceToHost, st));
+    chk(cudaMemcpyAsync(&flag, j.d_flag.p, 4, cudaMemcpyDeviceToHost, st));
+    chk(cudaStreamSynchronize(st));
+    if (s == GRN_OK && e == cudaSuccess && flag)
+      s = fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected a model record");
+  }
+  cudaFree(d_states.p);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "grn_evaluate_states");
+  return s;
+}
+
+grn_status grn_evaluate(grn_ctx *ctx, const grn_product *products, int n_products,
+                        const grn_link *links, int n_links, double max_error, double *error_out) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (!error_out || n_products < 0 || n_links < 0 || (n_products && !products) ||
+      (n_links && !links))
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad model");
+  const int32_t po[2] = {0, n_products}, lo[2] = {0, n_links};
+  grn_model_batch b{};
+  b.n_models = 1;
+  b.product_offsets = po;
+  b.products = products;
+  b.link_offsets = lo;
+  b.links = links;
+  return grn_evaluate_batch(ctx, &b, &max_error, error_out, nullptr, nullptr);
+}
+
+grn_status grn_submit(grn_ctx *ctx, int tag, const grn_model_batch *batch, const double *max_error,
+                      double *error_out, double *raw_error_out) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (!error_out && !raw_error_out)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "no output buffer");
+  cudaSetDevice(ctx->device);
+  Job *j;
+  if (!ctx->free_jobs.empty()) {
+    j = ctx->free_jobs.back();
+    ctx->free_jobs.pop_back();
+  } else {
+    j = new (std::nothrow) Job();
+    if (!j) return fail(ctx, GRN_ERR_OUT_OF_MEMORY, "job");
+  }
+  grn_status s = enqueue_job(ctx, j, batch, max_error, nullptr);
+  if (s != GRN_OK) {
+    ctx->free_jobs.push_back(j);
+    return s;
+  }
+  j->tag = tag;
+  j->error_out = error_out;
+  j->raw_out = raw_error_out;
+  j->max_error.assign(max_error, max_error + batch->n_models);
+  ctx->pending.push_back(j);
+  return GRN_OK;
+}
+
+grn_status grn_wait_any(grn_ctx *ctx, int timeout_ms, int *tag_out) {
+  if (!ctx || !tag_out) return GRN_ERR_INVALID_ARGUMENT;
+  if (ctx->pending.empty()) return fail(ctx, GRN_ERR_NOT_FOUND, "nothing submitted");
+  cudaSetDevice(ctx->device);
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    for (auto it = ctx->pending.begin(); it != ctx->pending.end(); ++it) {
+      Job *j = *it;
+      cudaError_t q = j->n_models ? cudaEventQuery(j->ev_done) : cudaSuccess;
+      if (q == cudaErrorNotReady) continue;
+      ctx->pending.erase(it);
+      ctx->free_jobs.push_back(j);
+      if (q != cudaSuccess) return cuda_fail(ctx, q, "cudaEventQuery");
+      *tag_out = j->tag;
+      return finish_job(ctx, j, j->max_error.data(), j->error_out, j->raw_out, nullptr);
+    }
+    if (timeout_ms >= 0) {
+      auto el = std::chrono::steady_clock::now() - t0;
+      if (std::chrono::duration<double, std::milli>(el).count() >= timeout_ms)
+        return fail(ctx, GRN_ERR_TIMEOUT, "no submitted batch finished in time");
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+grn_status grn_pack(grn_ctx *ctx, const grn_model_batch *batch, grn_packed **out) {
+  if (!ctx || !out) return GRN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  grn_status s = check_batch(ctx, batch);
+  if (s != GRN_OK) return s;
+  cudaSetDevice(ctx->device);
+  grn_packed *pk = new (std::nothrow) grn_packed();
+  if (!pk) return fail(ctx, GRN_ERR_OUT_OF_MEMORY, "packed");
+  pk->ctx = ctx;
+  std::string err;
+  s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      host_threads(), &pk->host, &err);
+  if (s != GRN_OK) {
+    delete pk;
+    return fail(ctx, s, err);
+  }
+  const size_t wb = std::max<size_t>(pk->host.words.size(), 1) * sizeof(uint4);
+  const size_t ob = std::max<size_t>(pk->host.offsets.size(), 1) * sizeof(int32_t);
+  if ((s = ensure_dev(ctx, &pk->d_words, wb)) || (s = ensure_dev(ctx, &pk->d_offsets, ob))) {
+    grn_packed_free(pk);
+    return s;
+  }
+  if (!pk->host.words.empty()) {
+    cudaMemcpy(pk->d_words.p, pk->host.words.data(), pk->host.words.size() * sizeof(uint4),
+               cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(pk->d_offsets.p, pk->host.offsets.data(),
+                               pk->host.offsets.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      grn_packed_free(pk);
+      return cuda_fail(ctx, e, "cudaMemcpy packed");
+    }
+  }
+  pk->cell_bound = (int64_t)batch->n_models * std::max(ctx->n_exp, 1) * ctx->p.num_sim_steps *
+                   ctx->p.dim_x * ctx->p.dim_y;
+  *out = pk;
+  return GRN_OK;
+}
+
+grn_status grn_packed_free(grn_packed *pk) {
+  if (!pk) return GRN_OK;
+  if (pk->ctx) cudaSetDevice(pk->ctx->device);
+  if (pk->d_words.p) cudaFree(pk->d_words.p);
+  if (pk->d_offsets.p) cudaFree(pk->d_offsets.p);
+  delete pk;
+  return GRN_OK;
+}
+
+grn_status grn_packed_get_info(const grn_packed *pk, grn_packed_info *info) {
+  if (!pk || !info) return GRN_ERR_INVALID_ARGUMENT;
+  std::memset(info, 0, sizeof *info);
+  const PackedHost &h = pk->host;
+  info->n_models = h.n_models;
+  info->device_bytes = (int64_t)(h.words.size() * sizeof(uint4) + h.offsets.size() * 4);
+  info->cell_update_bound = pk->cell_bound;
+  const int64_t cells = (int64_t)pk->ctx->p.dim_x * pk->ctx->p.dim_y;
+  info->sfu_ops_per_step = h.sfu_per_cell_step * cells;
+  info->max_genes = h.max_genes;
+  info->max_links = h.max_links;
+  info->mean_genes = h.n_models ? h.sum_genes / h.n_models : 0;
+  info->mean_links = h.n_models ? h.sum_links / h.n_models : 0;
+  return GRN_OK;
+}
+
+grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_max_error,
+                          double *d_raw_error, int32_t *d_steps, void *cuda_stream) {
+  if (!ctx || !pk || pk->ctx != ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (pk->host.n_models > 0 && (!d_max_error || !d_raw_error))
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null device pointer");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->stream;
+  grn_status s = ensure_dev(ctx, &ctx->sync_job.d_flag, 4);
+  if (s != GRN_OK) return s;
+  GRN_CUDA(ctx, cudaMemsetAsync(ctx->sync_job.d_flag.p, 0, 4, st));
+  return launch_packed(ctx, static_cast<const uint4 *>(pk->d_words.p),
+                       static_cast<const int32_t *>(pk->d_offsets.p), pk->host.n_models,
+                       pk->host.max_genes, d_max_error, d_raw_error, d_steps,
+                       static_cast<int32_t *>(ctx->sync_job.d_flag.p), st, nullptr);
+}
+
+}  // extern "C"
+
+extern "C" grn_status grn_describe_model(const grn_product *products, int n_products,
+                                         const grn_link *links, int n_links, int n_morphogens,
+                                         char *buf, int buf_len) {
+  if (!buf || buf_len < 1 || n_products < 0 || n_links < 0 || (n_products && !products) ||
+      (n_links && !links) || n_morphogens < 0)
+    return GRN_ERR_INVALID_ARGUMENT;
+  std::vector<uint4> rec;
+  grn::ModelCost cost;
+  std::string err;
+  grn_status s = grn::pack_model(products, n_products, links, n_links, n_morphogens, 0, &rec,
+                                 &cost, &err);
+  if (s != GRN_OK) return s;
+  grn::PackedHeader hdr;
+  std::memcpy(&hdr, rec.data(), sizeof hdr);
+  std::string out;
+  char line[256];
+  std::snprintf(line, sizeof line, "model genes %d links %d lg_mask %u\n", hdr.n_genes,
+                hdr.n_links, hdr.lg_mask);
+  out += line;
+  // Labels are the sorted labels in use; recompute them for the listing.
+  std::vector<int> labels;
+  for (int i = 0; i < n_morphogens; ++i) labels.push_back(i);
+  for (size_t h = 0; h < labels.size(); ++h)
+    for (int l = 0; l < n_links; ++l)
+      if (links[l].regulated == labels[h] &&
+          std::find(labels.begin(), labels.end(), links[l].regulator) == labels.end())
+        labels.push_back(links[l].regulator);
+  std::sort(labels.begin(), labels.end());
+  for (int i = 0; i < hdr.n_genes; ++i) {
+    grn::PackedGene g;
+    std::memcpy(&g, rec.data() + 1 + i, sizeof g);
+    std::snprintf(line, sizeof line, "gene %d label %d lim %.9g deg %.9g dif %.9g or %d and %d\n",
+                  i, labels[i], g.lim, g.deg, g.dif, g.n_or, g.n_and);
+    out += line;
+    for (int l = 0; l < g.n_or + g.n_and; ++l) {
+      grn::PackedLink k;
+      std::memcpy(&k, rec.data() + 1 + hdr.n_genes + g.link_begin + l, sizeof k);
+      std::snprintf(line, sizeof line, "link %d slot %d a %.9g b %.9g\n", i, k.slot, k.a, k.b);
+      out += line;
+    }
+  }
+  if ((int)out.size() + 1 > buf_len) return GRN_ERR_CAPACITY;
+  std::memcpy(buf, out.c_str(), out.size() + 1);
+  return GRN_OK;
+}

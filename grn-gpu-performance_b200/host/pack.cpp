@@ -1,0 +1,210 @@
+// pack.cpp -- host compiler from genome-form models to packed programs.
+#include "pack.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <thread>
+
+namespace grn {
+
+namespace {
+
+bool contains(const std::vector<int> &v, int x) {
+  return std::find(v.begin(), v.end(), x) != v.end();
+}
+
+}  // namespace
+
+grn_status pack_model(const grn_product *products, int n_products,
+                      const grn_link *links, int n_links, int n_morphogens,
+                      int orig_index, std::vector<uint4> *out,
+                      ModelCost *cost, std::string *err) {
+  // Labels in use: every morphogen, and every regulator of a label in use
+  // (Model::calcProductLabelsInUse, Src/Model/model.cpp:243-270).
+  std::vector<int> labels;
+  labels.reserve(16);
+  for (int i = 0; i < n_morphogens; ++i) labels.push_back(i);
+  for (size_t h = 0; h < labels.size(); ++h) {
+    const int lab = labels[h];
+    for (int l = 0; l < n_links; ++l)
+      if (links[l].regulated == lab && !contains(labels, links[l].regulator))
+        labels.push_back(links[l].regulator);
+    if ((int)labels.size() > GRN_MAX_GENES) {
+      if (err) *err = "model " + std::to_string(orig_index) + ": more than " +
+                      std::to_string(GRN_MAX_GENES) + " products in use";
+      return GRN_ERR_CAPACITY;
+    }
+  }
+  std::sort(labels.begin(), labels.end());  // qSort(labels_)
+  const int G = (int)labels.size();
+  auto index_of = [&](int lab) {
+    return (int)(std::lower_bound(labels.begin(), labels.end(), lab) - labels.begin());
+  };
+
+  PackedHeader hdr{};
+  hdr.orig_index = orig_index;
+  hdr.n_genes = (int16_t)G;
+  hdr.lg_mask = 0;
+  hdr.flags = kFlagNone;
+  std::vector<PackedGene> genes(G);
+  std::vector<PackedLink> plinks;
+  plinks.reserve(n_links);
+  ModelCost c;
+  c.genes = G;
+
+  for (int i = 0; i < G; ++i) {
+    // Model::prodWithLabel: first product with the label (model.cpp:227-240).
+    const grn_product *prod = nullptr;
+    for (int p = 0; p < n_products; ++p)
+      if (products[p].label == labels[i]) {
+        prod = &products[p];
+        break;
+      }
+    if (!prod) {
+      if (err) *err = "model " + std::to_string(orig_index) + ": label " +
+                      std::to_string(labels[i]) + " is in use but has no product";
+      return GRN_ERR_MODEL;
+    }
+    PackedGene &g = genes[i];
+    g.lim = (float)prod->lim;
+    g.deg = (float)prod->deg;
+    // The product diffuses iff dif > 0 (cmodelsimulator.cpp:143-147).
+    g.dif = prod->dif > 0 ? (float)prod->dif : 0.0f;
+    if (g.dif > 0) ++c.dif_genes;
+
+    // OR links first, then AND links, each in model link order; a link is
+    // used if its regulator is in use (cmodelsimulator.cpp:150-167).
+    bool any_activator = false;
+    std::vector<const grn_link *> or_l, and_l;
+    for (int l = 0; l < n_links; ++l) {
+      const grn_link &lk = links[l];
+      if (lk.regulated != labels[i]) continue;
+      if (std::binary_search(labels.begin(), labels.end(), lk.regulator)) {
+        if (lk.is_and) and_l.push_back(&lk);
+        else or_l.push_back(&lk);
+      }
+      if (lk.hill_coef >= 0) any_activator = true;
+    }
+    g.link_begin = (uint16_t)plinks.size();
+    g.n_or = 0;
+    g.n_and = 0;
+    // No activator at all: regulation 0 (OpZero, cmodelsimulator.cpp:168-172);
+    // no used link: also 0 (:216-217).
+    if (!any_activator) continue;
+    auto emit = [&](const grn_link *lk) {
+      PackedLink pl{};
+      // createHillOpForLink (cmodelsimulator.cpp:221-227): hillCoef >= 0 is
+      // activation with n = hillCoef, else repression with n = -hillCoef.
+      const bool act = lk->hill_coef >= 0;
+      const double n = act ? lk->hill_coef : -1.0 * lk->hill_coef;
+      if (n == 0) {
+        pl.slot = kConstSlot;  // pow(x, 0) = pow(K, 0) = 1: Hill value 1/2
+        pl.a = 0.0f;
+        pl.b = 0.0f;
+      } else {
+        const double lk2 = std::log2(lk->dis_const);
+        pl.slot = index_of(lk->regulator);
+        pl.a = (float)(act ? -n : n);
+        pl.b = (float)(act ? n * lk2 : -n * lk2);
+        hdr.lg_mask |= 1u << pl.slot;
+      }
+      plinks.push_back(pl);
+    };
+    for (const grn_link *lk : or_l) emit(lk);
+    for (const grn_link *lk : and_l) emit(lk);
+    g.n_or = (uint8_t)or_l.size();
+    g.n_and = (uint8_t)and_l.size();
+    if ((int)plinks.size() > GRN_MAX_LINKS || or_l.size() > 255 || and_l.size() > 255) {
+      if (err) *err = "model " + std::to_string(orig_index) + ": more than " +
+                      std::to_string(GRN_MAX_LINKS) + " used links";
+      return GRN_ERR_CAPACITY;
+    }
+    if (g.n_or + g.n_and > 0) ++c.reg_genes;
+  }
+  hdr.n_links = (int16_t)plinks.size();
+  c.links = (int)plinks.size();
+  c.lg_genes = __builtin_popcount(hdr.lg_mask);
+  // Relative cost of one cell-step: MUFU ops weigh 8 issue slots' worth of
+  // pipe time, a link ~5 instructions, a gene ~16.
+  c.cost = 8.0 * (c.lg_genes + 2 * c.reg_genes) / 4.0 + 5.0 * c.links + 16.0 * G;
+
+  const size_t w0 = out->size();
+  out->resize(w0 + record_words(G, (int)plinks.size()));
+  uint4 *w = out->data() + w0;
+  std::memcpy(w, &hdr, sizeof hdr);
+  if (G) std::memcpy(w + 1, genes.data(), sizeof(PackedGene) * G);
+  if (!plinks.empty())
+    std::memcpy(w + 1 + G, plinks.data(), sizeof(PackedLink) * plinks.size());
+  if (cost) *cost = c;
+  return GRN_OK;
+}
+
+grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
+                      int n_threads, PackedHost *out, std::string *err) {
+  const int n = batch->n_models;
+  std::vector<std::vector<uint4>> recs(n);
+  std::vector<ModelCost> costs(n);
+  std::atomic<int> next{0};
+  std::atomic<int> status{GRN_OK};
+  std::string first_err;
+  std::atomic<bool> err_taken{false};
+  auto worker = [&]() {
+    for (;;) {
+      const int m = next.fetch_add(1);
+      if (m >= n || status.load() != GRN_OK) break;
+      const int p0 = batch->product_offsets[m], p1 = batch->product_offsets[m + 1];
+      const int l0 = batch->link_offsets[m], l1 = batch->link_offsets[m + 1];
+      std::string e;
+      grn_status s = pack_model(batch->products + p0, p1 - p0, batch->links + l0,
+                                l1 - l0, n_morphogens, m, &recs[m], &costs[m], &e);
+      if (s != GRN_OK) {
+        bool expected = false;
+        if (err_taken.compare_exchange_strong(expected, true)) first_err = e;
+        status.store(s);
+      }
+    }
+  };
+  if (n_threads < 1) n_threads = 1;
+  if (n < 256) n_threads = 1;
+  n_threads = std::min(n_threads, 16);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < n_threads; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  if (status.load() != GRN_OK) {
+    if (err) *err = first_err;
+    return (grn_status)status.load();
+  }
+
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return costs[a].cost > costs[b].cost; });
+  size_t total = 0;
+  for (int m = 0; m < n; ++m) total += recs[m].size();
+  out->words.clear();
+  out->words.reserve(total);
+  out->offsets.resize(n);
+  out->n_models = n;
+  out->max_genes = out->max_links = 0;
+  out->sum_genes = out->sum_links = 0;
+  out->sfu_per_cell_step = out->fma_per_cell_step = 0;
+  for (int i = 0; i < n; ++i) {
+    const int m = order[i];
+    out->offsets[i] = (int32_t)out->words.size();
+    out->words.insert(out->words.end(), recs[m].begin(), recs[m].end());
+    const ModelCost &c = costs[m];
+    out->max_genes = std::max(out->max_genes, c.genes);
+    out->max_links = std::max(out->max_links, c.links);
+    out->sum_genes += c.genes;
+    out->sum_links += c.links;
+    out->sfu_per_cell_step += c.lg_genes + 2 * c.reg_genes;
+    out->fma_per_cell_step += 2 * c.links + 6 * c.genes + 6 * c.dif_genes;
+  }
+  return GRN_OK;
+}
+
+}  // namespace grn

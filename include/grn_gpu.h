@@ -1,0 +1,317 @@
+/*
+ * grn_gpu.h -- C ABI of the B200 GRN fitness evaluator.
+ *
+ * The evaluator batch-simulates spatial gene-regulatory-network (GRN)
+ * reaction-diffusion models with explicit Euler steps on a 2-D grid and scores
+ * every model against target expression patterns.  It replaces the GPU
+ * evaluator of lobolab/grn-gpu-performance (directory Src/GPUSimulator) and
+ * keeps that evaluator's observable behaviour:
+ *
+ *   reference entry point                               replacement
+ *   ---------------------------------------------------  -------------------------
+ *   CEvaluatorMorphogens(threadId, search)               grn_create
+ *     (Src/GPUSimulator/cevaluatormorphogens.cpp:35-56)
+ *   createGPUExperimentDataset / copySimState            grn_set_experiments,
+ *     (cevaluatormorphogens.cpp:92-182)                    grn_set_experiments_rgb
+ *   CEvaluatorMorphogens::evaluate(model, maxError)      grn_evaluate
+ *     (cevaluatormorphogens.cpp:233-245)
+ *   CModelSimulator::loadModel + simulateExperiment      grn_pack + grn_run_packed
+ *     (Src/GPUSimulator/cmodelsimulator.cpp:114-242)
+ *   launchKernel (modelsimulatordevice.cu:253-264)       grn_run_packed
+ *   ErrorCalculator::process / waitForAnyDeme            grn_submit / grn_wait_any
+ *     (Src/Search/errorcalculator.h:19-20)
+ *   ~CEvaluatorMorphogens                                grn_destroy
+ *
+ * Conventions
+ *   - Every function returns a grn_status; nothing aborts the process.  The
+ *     reference aborts on any CUDA error (cerrorhandle.h:21); here the caller
+ *     decides.  grn_last_error(ctx) gives a one-line description.
+ *   - Input buffers are owned by the caller and copied; nothing is retained
+ *     after the call returns (except by grn_submit, see there).
+ *   - One context per host thread, or external locking.  A context owns one
+ *     CUDA stream on one device, like the reference's one evaluator per GPU
+ *     worker thread (errorcalculatormultithread.cpp:233-254).
+ *   - Grids are planar, row-major: value (x, y) of channel k lives at
+ *     [k][y][x] with x < dim_x (width) fastest.  This is the memory order of
+ *     the reference CPU simulator's Eigen matrices product(k)(x, y)
+ *     (Src/Simulator/modelsimulator.cpp:213-216).
+ *   - The product path has no CPU fallback: if no CUDA device is usable,
+ *     grn_create returns GRN_ERR_NO_DEVICE.
+ */
+#ifndef GRN_GPU_H_
+#define GRN_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRN_ABI_VERSION 1
+
+/* Capacity limits of the compiled model format.  A model whose products in
+ * use or used links exceed these is rejected with GRN_ERR_CAPACITY. */
+#define GRN_MAX_GENES 16         /* products in use per model              */
+#define GRN_MAX_LINKS 128        /* links from an in-use regulator         */
+#define GRN_MAX_INPUT_MORPHOGENS 3  /* R, G, B channels of an input image  */
+#define GRN_MAX_EXPERIMENTS 64
+
+typedef enum grn_status {
+  GRN_OK = 0,
+  GRN_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad params     */
+  GRN_ERR_NO_DEVICE = 2,        /* no CUDA device / bad device ordinal    */
+  GRN_ERR_CUDA = 3,             /* a CUDA runtime call failed             */
+  GRN_ERR_OUT_OF_MEMORY = 4,    /* device or pinned host allocation       */
+  GRN_ERR_MODEL = 5,            /* incoherent model (missing product ...) */
+  GRN_ERR_CAPACITY = 6,         /* model or grid exceeds the kernel limits */
+  GRN_ERR_NO_EXPERIMENTS = 7,   /* evaluate before grn_set_experiments    */
+  GRN_ERR_TIMEOUT = 8,          /* grn_wait_any ran out of time           */
+  GRN_ERR_NOT_FOUND = 9,        /* grn_wait_any with nothing submitted    */
+  GRN_ERR_KERNEL = 10           /* the kernel reported an internal error  */
+} grn_status;
+
+/* Per-experiment distance between the simulated and the target pattern. */
+typedef enum grn_fitness_kind {
+  /* The reference's thresholded log distance:
+   *   (1/(W*H)) * sum_cells sum_k [|c - t| - theta > 0] * log(1 + |c - t| - theta)
+   * (Src/Simulator/simstate.cpp:135-158).  Use this for drop-in parity.     */
+  GRN_FITNESS_REF_LOGTHRESH = 0,
+  /* Mean squared error over cells and target channels:
+   *   (1/(W*H*nTarget)) * sum_cells sum_k (c - t)^2
+   * No reference counterpart; the rest of the evaluation (non-convergence
+   * penalty, maxError abandon, rounding) is unchanged.                     */
+  GRN_FITNESS_MSE = 1
+} grn_fitness_kind;
+
+/* Simulation parameters: the fields of the reference SimParams that the
+ * fitness path reads (Src/Simulator/simparams.h:25-43). */
+typedef struct grn_sim_params {
+  int32_t dim_x;                /* SimParams::size.width()                */
+  int32_t dim_y;                /* SimParams::size.height()               */
+  int32_t n_input_morphogens;   /* SimParams::nInputMorphogens            */
+  int32_t n_target_morphogens;  /* SimParams::nTargetMorphogens           */
+  int32_t num_sim_steps;        /* SimParams::NumSimSteps (max Euler steps) */
+  int32_t error_precision;      /* SimParams::errorPrecision (sig. digits) */
+  int32_t fitness_kind;         /* grn_fitness_kind                       */
+  int32_t reserved0;
+  double dt;                    /* SimParams::dt                          */
+  double min_conc;              /* SimParams::minConc                     */
+  double min_conc_change;       /* SimParams::minConcChange               */
+  double dist_error_threshold;  /* SimParams::distErrorThreshold          */
+} grn_sim_params;
+
+/* One gene product of a model (reference ModelProd, Src/Model/modelprod.h). */
+typedef struct grn_product {
+  int32_t label;   /* product label; labels 0..nMorphogens-1 are morphogens */
+  int32_t reserved0;
+  double init;     /* ModelProd::init (not read by the simulation)          */
+  double lim;      /* production rate                                       */
+  double deg;      /* degradation rate                                      */
+  double dif;      /* diffusion constant; the product diffuses iff dif > 0  */
+} grn_product;
+
+/* One regulatory link (reference ModelLink, Src/Model/modellink.h). */
+typedef struct grn_link {
+  int32_t regulator;   /* label of the regulating product                  */
+  int32_t regulated;   /* label of the regulated product                   */
+  double dis_const;    /* Hill dissociation constant K                     */
+  double hill_coef;    /* Hill coefficient n; n < 0 means repression       */
+  int32_t is_and;      /* 1 = AND regulation, 0 = OR regulation            */
+  int32_t reserved0;
+} grn_link;
+
+/* A batch of models in genome form: model m owns products
+ * [product_offsets[m], product_offsets[m+1]) and links
+ * [link_offsets[m], link_offsets[m+1]); both offset arrays have n_models+1
+ * entries and start at 0.  Link order inside a model is significant (it is
+ * the order of the reference's Model::links_). */
+typedef struct grn_model_batch {
+  int32_t n_models;
+  int32_t reserved0;
+  const int32_t *product_offsets;
+  const grn_product *products;
+  const int32_t *link_offsets;
+  const grn_link *links;
+} grn_model_batch;
+
+/* Optional statistics of one evaluation call. */
+typedef struct grn_eval_stats {
+  int64_t n_models;
+  int64_t cell_updates;      /* sum over models of steps run x W x H      */
+  int64_t total_steps;       /* Euler steps run, summed over models/exps  */
+  double kernel_ms;          /* device time of the simulation kernel(s)   */
+  double pack_ms;            /* host time compiling the batch             */
+  int64_t h2d_bytes;         /* bytes copied host -> device               */
+  int64_t d2h_bytes;         /* bytes copied device -> host               */
+  int32_t schedule;          /* grn_schedule chosen for the launch        */
+  int32_t threads_per_block;
+  int32_t blocks;
+  int32_t reserved0;
+} grn_eval_stats;
+
+/* Kernel schedules.  GRN_SCHEDULE_AUTO lets the autotuner pick. */
+typedef enum grn_schedule {
+  GRN_SCHEDULE_AUTO = 0,
+  GRN_SCHEDULE_SMEM_1BUF = 1,  /* one CTA per model, state in shared memory,
+                                  new values held in registers            */
+  GRN_SCHEDULE_SMEM_2BUF = 2,  /* one CTA per model, double-buffered state
+                                  in shared memory                        */
+  GRN_SCHEDULE_GLOBAL = 3      /* one CTA per model, double-buffered state
+                                  in global memory (grids too large for
+                                  shared memory)                          */
+} grn_schedule;
+
+typedef struct grn_ctx grn_ctx;
+typedef struct grn_packed grn_packed;
+
+/* ---------------------------------------------------------------- context */
+
+/* Creates an evaluator bound to CUDA device `device` with its own stream.
+ * Mirrors CEvaluatorMorphogens' constructor (cevaluatormorphogens.cpp:35-56,
+ * 64-90), minus the experiment upload, which is grn_set_experiments. */
+grn_status grn_create(grn_ctx **out, int device, const grn_sim_params *params);
+
+/* Frees every device and pinned buffer of the context.  Mirrors
+ * ~CEvaluatorMorphogens (cevaluatormorphogens.cpp:193-231).  NULL is a no-op. */
+grn_status grn_destroy(grn_ctx *ctx);
+
+/* Description of the last error on this context ("" if none). */
+const char *grn_last_error(const grn_ctx *ctx);
+
+/* Name of a status code. */
+const char *grn_status_str(grn_status status);
+
+/* ABI version compiled into the library (GRN_ABI_VERSION). */
+int grn_abi_version(void);
+
+/* Forces a schedule instead of the autotuner's choice (GRN_SCHEDULE_AUTO to
+ * restore).  Returns GRN_ERR_CAPACITY later, at launch, if the forced
+ * schedule cannot hold the batch. */
+grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block);
+
+/* ------------------------------------------------------------ experiments */
+
+/* Uploads the experiments once (the reference uploads them once per device,
+ * cevaluatormorphogens.cpp:92-151).
+ *   initial: [n_experiments][n_input_morphogens][dim_y][dim_x]
+ *   target:  [n_experiments][n_target_morphogens][dim_y][dim_x]
+ * Products other than the input morphogens start at 0
+ * (Src/Simulator/simstate.cpp:64-69, modelsimulatordevice.cu:134-151). */
+grn_status grn_set_experiments(grn_ctx *ctx, int n_experiments,
+                               const double *initial, const double *target);
+
+/* Same, from 32-bit 0xAARRGGBB pixels (Qt's QRgb), scanline-major
+ * [n_experiments][dim_y][dim_x], the form the reference decodes with QImage.
+ * Channel k takes byte (16 - 8k) / 255 and the y axis is flipped, exactly as
+ * SimState::loadMorphologyImage (Src/Simulator/simstate.cpp:71-90). */
+grn_status grn_set_experiments_rgb(grn_ctx *ctx, int n_experiments,
+                                   const uint32_t *input_pixels,
+                                   const uint32_t *target_pixels);
+
+/* Decodes 0xAARRGGBB pixels [dim_y][dim_x] into planar channels
+ * [n_channels][dim_y][dim_x] with the reference's y flip.  Pure host helper
+ * (no device work), exposed so callers can check the decode. */
+grn_status grn_decode_rgb(int dim_x, int dim_y, int n_channels,
+                          const uint32_t *pixels, double *out);
+
+/* -------------------------------------------------------------- evaluate */
+
+/* Evaluates one model synchronously and returns the reference's fitness:
+ * 100 if the error exceeds max_error, else the error rounded UP to
+ * error_precision significant digits.  Mirrors
+ * CEvaluatorMorphogens::evaluate (cevaluatormorphogens.cpp:233-245). */
+grn_status grn_evaluate(grn_ctx *ctx, const grn_product *products,
+                        int n_products, const grn_link *links, int n_links,
+                        double max_error, double *error_out);
+
+/* Evaluates a batch synchronously in one persistent launch.
+ *   max_error:     [n_models] (the parent's error; 1000 for random models)
+ *   error_out:     [n_models] rounded fitness as grn_evaluate returns it
+ *   raw_error_out: [n_models] unrounded error sum, or NULL
+ *   stats:         optional */
+grn_status grn_evaluate_batch(grn_ctx *ctx, const grn_model_batch *batch,
+                              const double *max_error, double *error_out,
+                              double *raw_error_out, grn_eval_stats *stats);
+
+/* Evaluates a batch like grn_evaluate_batch and also returns the final
+ * simulated state of every experiment of every model -- the state that
+ * SimState::negativeLogLikelihood scores (Src/Simulator/simstate.cpp:135-158)
+ * -- for inspection and headless viewers:
+ *   states_out: [n_models][n_experiments][max_planes][dim_y][dim_x] FP32,
+ *               plane k = product index k (sorted labels in use); planes
+ *               beyond a model's products and experiments skipped after
+ *               max_error stay 0.
+ *   raw_error_out: [n_models] unrounded errors (may be NULL). */
+grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch,
+                               const double *max_error, double *raw_error_out,
+                               float *states_out, int max_planes);
+
+/* Asynchronous form of grn_evaluate_batch, the reference's
+ * ErrorCalculator::process(iDeme, individuals) (errorcalculator.h:19).
+ * The batch is compiled and copied before the call returns; error_out
+ * (and raw_error_out if not NULL) must stay valid until grn_wait_any has
+ * returned `tag`. */
+grn_status grn_submit(grn_ctx *ctx, int tag, const grn_model_batch *batch,
+                      const double *max_error, double *error_out,
+                      double *raw_error_out);
+
+/* Blocks until one submitted batch has finished, writes its results and
+ * returns its tag: ErrorCalculator::waitForAnyDeme (errorcalculator.h:20).
+ * timeout_ms < 0 waits without limit.  GRN_ERR_NOT_FOUND if nothing is
+ * pending, GRN_ERR_TIMEOUT if nothing finished in time. */
+grn_status grn_wait_any(grn_ctx *ctx, int timeout_ms, int *tag_out);
+
+/* --------------------------------------------------- device-level API ---
+ * For callers that keep inputs resident on the device (CUDA graphs,
+ * benchmarks).  grn_pack compiles a batch into the packed program format
+ * (host work, CModelSimulator::loadModel for every model) and copies it to
+ * device memory owned by the returned handle. */
+grn_status grn_pack(grn_ctx *ctx, const grn_model_batch *batch,
+                    grn_packed **out);
+grn_status grn_packed_free(grn_packed *packed);
+
+typedef struct grn_packed_info {
+  int64_t n_models;
+  int64_t device_bytes;      /* size of the packed program on the device */
+  int64_t cell_update_bound; /* n_models * n_experiments * steps * W * H  */
+  int64_t sfu_ops_per_step;  /* MUFU ops of one Euler step of all models  */
+  int32_t max_genes;         /* largest products-in-use count             */
+  int32_t max_links;         /* largest used-link count                   */
+  double mean_genes;
+  double mean_links;
+} grn_packed_info;
+grn_status grn_packed_get_info(const grn_packed *packed, grn_packed_info *info);
+
+/* Launches the simulation of a packed batch on `cuda_stream` (a
+ * cudaStream_t; NULL = the context's stream) and returns without waiting.
+ * All pointers are device pointers of n_models entries:
+ *   d_max_error (in), d_raw_error (out, unrounded error),
+ *   d_steps (out, Euler steps run summed over experiments; may be NULL). */
+grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *packed,
+                          const double *d_max_error, double *d_raw_error,
+                          int32_t *d_steps, void *cuda_stream);
+
+/* Compiles one model on the host, as grn_pack does, and writes a text
+ * listing of its program (no device work):
+ *   "model genes G links L lg_mask M\n"
+ *   "gene i label LABEL lim LIM deg DEG dif DIF or N_OR and N_AND\n"  (per gene)
+ *   "link i slot S a A b B\n"  (per link of gene i, OR links first)
+ * Exponent form: a link's Hill value is 1 / (1 + 2^(a*lg2(x) + b)); slot 255
+ * is the constant slot of a Hill coefficient 0.  Mirrors the op list the
+ * reference builds in CModelSimulator::loadModel
+ * (Src/GPUSimulator/cmodelsimulator.cpp:114-227). */
+grn_status grn_describe_model(const grn_product *products, int n_products,
+                              const grn_link *links, int n_links,
+                              int n_morphogens, char *buf, int buf_len);
+
+/* Rounds a raw error the way the reference's evaluate does:
+ * 100 if raw > max_error, else ceilS(raw, precision)
+ * (Src/Common/mathalgo.h:55-62). */
+double grn_round_error(double raw_error, double max_error, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRN_GPU_H_ */

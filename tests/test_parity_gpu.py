@@ -1,0 +1,326 @@
+"""GPU parity tests: the CUDA path, called through the C ABI, against the
+FP64 oracle on the same seeded inputs.
+
+Tolerance: the kernels keep FP32 state and use the MUFU lg2/ex2/rcp
+approximations; the oracle is FP64.  Raw (unrounded) errors must agree to
+RTOL = 1e-4 relative (ATOL = 1e-7 absolute for errors near zero), rounded
+errors to the same tolerance or one unit of the last rounded digit, and the
+selection ranking of ties-free populations must be identical.  Different
+kernel schedules run the same arithmetic and must agree bit for bit.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import binding as oracle
+import grn_b200 as grn
+import synth
+from grn_b200 import LINK_DTYPE, PRODUCT_DTYPE, ModelBatch
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+ATOL = 1e-7
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def assert_raw_close(gpu, ref, rtol=RTOL, atol=ATOL, what=""):
+    gpu, ref = np.asarray(gpu), np.asarray(ref)
+    both_nan = np.isnan(gpu) & np.isnan(ref)
+    ok = both_nan | (np.abs(gpu - ref) <= atol + rtol * np.abs(ref))
+    if not ok.all():
+        bad = np.where(~ok)[0]
+        rel = np.abs(gpu - ref) / np.maximum(np.abs(ref), 1e-300)
+        raise AssertionError("%s: %d/%d outside tolerance, worst rel %.3g at %d (gpu %r ref %r)"
+                             % (what, len(bad), len(ok), rel[bad].max(), bad[rel[bad].argmax()],
+                                gpu[bad[rel[bad].argmax()]], ref[bad[rel[bad].argmax()]]))
+
+
+def assert_rounded_close(gpu, ref, precision):
+    for g, r in zip(gpu, ref):
+        if r == 100.0 or g == 100.0:
+            assert g == r
+            continue
+        unit = 10.0 ** (math.ceil(math.log10(abs(r))) - precision) if r else 0.0
+        assert abs(g - r) <= max(unit * 1.001, ATOL + RTOL * abs(r)), (g, r)
+
+
+def assert_same_ranking(gpu, ref, rtol=2 * RTOL):
+    """Pairs the oracle separates by more than the tolerance keep their order."""
+    gpu, ref = np.asarray(gpu), np.asarray(ref)
+    o = np.argsort(ref, kind="stable")
+    r, g = ref[o], gpu[o]
+    for i in range(len(r) - 1):
+        for j in range(i + 1, len(r)):
+            if r[j] - r[i] > rtol * max(abs(r[i]), abs(r[j])) + ATOL:
+                assert g[i] < g[j], (o[i], o[j], r[i], r[j], g[i], g[j])
+
+
+def run_both(params, batch, init, tgt, max_error=None, schedule=None, threads=None):
+    with grn.Evaluator(params) as ev:
+        if schedule is not None:
+            ev.set_schedule(schedule)
+        ev.set_experiments(init, tgt)
+        err, raw, stats = ev.evaluate_batch(batch, max_error)
+    oe, oraw, osteps = oracle.evaluate_batch(params, init, tgt, batch, max_error, n_threads=threads)
+    return err, raw, stats, oe, oraw, osteps
+
+
+def load_golden():
+    with open(os.path.join(GOLDEN, "oracle_small.json")) as f:
+        cases = json.load(f)["cases"]
+    out = []
+    for c in cases:
+        batch = ModelBatch(c["product_offsets"],
+                           np.array([tuple(r) for r in c["products"]], PRODUCT_DTYPE),
+                           c["link_offsets"], np.array([tuple(r) for r in c["links"]], LINK_DTYPE))
+        out.append((c, batch))
+    return out
+
+
+@pytest.mark.parametrize("W,H,steps", [(8, 8, 1), (8, 8, 30), (13, 5, 40), (64, 64, 50)])
+def test_final_states_match_oracle(W, H, steps):
+    """Final simulated state planes against the oracle's, cell by cell."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=W * H + steps, n_models=12,
+                                              steps=steps, W=W, H=H)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        raw, states = ev.evaluate_states(batch, max_planes=16)
+    for m in range(batch.n_models):
+        pr, li = batch.model(m)
+        ref, _, _ = oracle.simulate(params, init[0], pr, li, steps)
+        got = states[m, 0, :len(ref)].astype(np.float64)
+        err = np.abs(got - ref)
+        tol = 1e-6 + 1e-4 * np.abs(ref)
+        if not (err <= tol).all():
+            k, y, x = np.unravel_index(np.argmax(err - tol), err.shape)
+            raise AssertionError("model %d: gene %d cell (%d,%d): gpu %r oracle %r (%d genes)"
+                                 % (m, k, x, y, got[k, y, x], ref[k, y, x], len(ref)))
+
+
+def test_golden_fixtures():
+    for c, batch in load_golden():
+        p = c["params"]
+        with grn.Evaluator(p) as ev:
+            ev.set_experiments(np.array(c["initial"]), np.array(c["target"]))
+            err, raw, stats = ev.evaluate_batch(batch, c["max_error"])
+        assert_raw_close(raw, c["raw_error"], what="golden %dx%d" % (p["dim_x"], p["dim_y"]))
+        assert_rounded_close(err, c["error"], p["error_precision"])
+
+
+def test_small_32x32_full_config():
+    """64 models, 3 genes, 32x32, 500 steps, MSE fitness: the CPU-runnable
+    configuration at full size."""
+    params, batch, init, tgt = synth.workload("small_32x32", seed=1)
+    err, raw, stats, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="small_32x32")
+    assert_rounded_close(err, oe, params["error_precision"])
+    assert_same_ranking(raw, oraw)
+    assert stats["cell_updates"] == 64 * 500 * 32 * 32
+
+
+def test_small_32x32_ref_fitness():
+    params, batch, init, tgt = synth.workload("small_32x32", seed=2, fitness=0)
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="small_32x32 logthresh")
+    assert_same_ranking(raw, oraw)
+
+
+def test_uneven_64x64_sample():
+    """Uneven 2-8 genes / 1-24 links at 64x64 (the headline grid)."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=3, n_models=40, steps=300)
+    err, raw, stats, oe, oraw, osteps = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="uneven_64x64")
+    assert_same_ranking(raw, oraw)
+
+
+def test_uneven_64x64_full_steps_sample():
+    """A few models of the headline workload at the full 2000 steps."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=4, n_models=6)
+    err, raw, stats, oe, oraw, osteps = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="uneven_64x64 2000 steps")
+
+
+@pytest.mark.parametrize("W,H", [(10, 7), (13, 1), (1, 13), (1, 1), (33, 17), (5, 64), (64, 3)])
+def test_ragged_grids(W, H):
+    """Widths that are not multiples of 4, single rows/columns, 1x1."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=W * 100 + H, n_models=24,
+                                              steps=120, W=W, H=H)
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="%dx%d" % (W, H))
+
+
+@pytest.mark.parametrize("W,H,steps", [(100, 100, 40), (256, 256, 12), (140, 90, 30)])
+def test_large_grids(W, H, steps):
+    """Grids that do not fit shared memory at 8 genes (hybrid / global)."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=W + H, n_models=10,
+                                              steps=steps, W=W, H=H, genes=(6, 8))
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="%dx%d" % (W, H))
+
+
+def test_schedules_agree_bitwise():
+    """Double-buffered, register-held and global-memory schedules compute
+    identical results."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=5, n_models=30, steps=80,
+                                              W=36, H=20)
+    outs = {}
+    for sched in (grn.SCHEDULE_AUTO, grn.SCHEDULE_SMEM_2BUF, grn.SCHEDULE_SMEM_1BUF,
+                  grn.SCHEDULE_GLOBAL):
+        with grn.Evaluator(params) as ev:
+            ev.set_schedule(sched)
+            ev.set_experiments(init, tgt)
+            _, raw, st = ev.evaluate_batch(batch)
+        outs[sched] = (raw, st["schedule"])
+    base = outs[grn.SCHEDULE_AUTO][0]
+    for sched, (raw, used) in outs.items():
+        assert np.array_equal(raw, base), (sched, used)
+    oe, oraw, _ = oracle.evaluate_batch(params, init, tgt, batch)
+    assert_raw_close(base, oraw, what="schedules")
+
+
+def test_early_exit_and_steps():
+    """minConcChange stops simulations early; the non-convergence penalty
+    uses the running change sum."""
+    params, batch, init, tgt = synth.workload("small_32x32", seed=6, n_models=32, steps=3000,
+                                              min_conc_change=1e-3, fitness=0, n_exp=2)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        err, raw, stats = ev.evaluate_batch(batch)
+    oe, oraw, osteps = oracle.evaluate_batch(params, init, tgt, batch)
+    assert_raw_close(raw, oraw, rtol=1e-3, what="early exit")
+    assert stats["total_steps"] < 32 * 2 * 3000  # something converged
+
+
+def test_max_error_abandon():
+    params, batch, init, tgt = synth.workload("small_32x32", seed=7, n_models=32, steps=100,
+                                              n_exp=3, fitness=0)
+    _, _, _, _, oraw, _ = run_both(params, batch, init, tgt)
+    # parents' errors: half the models get a bound below their own error
+    me = np.where(np.arange(32) % 2 == 0, oraw * 0.5, 1000.0)
+    err, raw, _, oe, oraw2, _ = run_both(params, batch, init, tgt, max_error=me)
+    assert np.array_equal(err == 100.0, oe == 100.0)
+    assert (err[::2] == 100.0).all()
+    assert_rounded_close(err, oe, params["error_precision"])
+
+
+def test_edge_models():
+    """Zero regulation (no activator), Hill coefficient 0, K = 0 (NaN Hill
+    values at x = 0, which the reference propagates), duplicate links."""
+    rng = np.random.default_rng(8)
+    models = []
+    for t in range(24):
+        pr, li = synth.random_model(rng, 4, 8, 2)
+        if t % 4 == 0:
+            li["hill_coef"] = -np.abs(li["hill_coef"])  # no activator anywhere
+        if t % 4 == 1:
+            li["hill_coef"][:3] = 0.0
+        if t % 4 == 2:
+            li["dis_const"][:2] = 0.0
+        if t % 4 == 3:
+            li = np.concatenate([li, li[:2]])
+        models.append((pr, li))
+    batch = ModelBatch.from_models(models)
+    params, _, init, tgt = synth.workload("small_32x32", seed=9, n_models=1, steps=150, fitness=0,
+                                          n_target=1, W=12, H=9)
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="edge models")
+
+
+def test_reference_test_model():
+    """The reference's built-in test model (13 products, 19 links) on
+    synthetic patterns with 2 morphogens."""
+    with open(os.path.join(GOLDEN, "reference_test_model.json")) as f:
+        pr, li = oracle.parse_model(json.load(f)["model"])
+    batch = ModelBatch.from_models([(pr, li)] * 4)
+    params, _, init, tgt = synth.workload("small_32x32", seed=10, n_models=1, steps=400,
+                                          n_target=1, fitness=0, n_exp=2)
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt)
+    assert_raw_close(raw, oraw, what="reference test model")
+    assert len(set(raw.tolist())) == 1
+
+
+def test_single_evaluate_matches_batch():
+    params, batch, init, tgt = synth.workload("small_32x32", seed=11, n_models=8, steps=60)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        err, raw, _ = ev.evaluate_batch(batch, 1000.0)
+        singles = [ev.evaluate(*batch.model(i), 1000.0) for i in range(batch.n_models)]
+    assert np.array_equal(np.array(singles), err)
+
+
+def test_submit_wait_any():
+    """ErrorCalculator::process / waitForAnyDeme semantics."""
+    params, batch, init, tgt = synth.workload("small_32x32", seed=12, n_models=40, steps=80)
+    demes = [batch.subset(range(i * 10, (i + 1) * 10)) for i in range(4)]
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ref = [ev.evaluate_batch(d)[0] for d in demes]
+        for i, d in enumerate(demes):
+            ev.submit(i, d)
+        seen = set()
+        for _ in range(4):
+            tag, err, raw = ev.wait_any(timeout_ms=60000)
+            assert tag not in seen
+            seen.add(tag)
+            assert np.array_equal(err, ref[tag])
+        with pytest.raises(grn.GrnError) as e:
+            ev.wait_any(timeout_ms=10)
+        assert e.value.status == 9
+
+
+def test_rgb_experiments_match_planar():
+    rng = np.random.default_rng(13)
+    params, batch, _, _ = synth.workload("small_32x32", seed=13, n_models=6, steps=50, n_target=1)
+    W, H = params["dim_x"], params["dim_y"]
+    pin = rng.integers(0, 2 ** 32, size=(2, H, W), dtype=np.uint64).astype(np.uint32)
+    pout = rng.integers(0, 2 ** 32, size=(2, H, W), dtype=np.uint64).astype(np.uint32)
+    init = np.stack([grn.decode_rgb(p, 1) for p in pin])
+    tgt = np.stack([grn.decode_rgb(p, 1) for p in pout])
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments_rgb(pin, pout)
+        a = ev.evaluate_batch(batch)[1]
+        ev.set_experiments(init, tgt)
+        b = ev.evaluate_batch(batch)[1]
+    assert np.array_equal(a, b)
+
+
+def test_run_packed_device_buffers():
+    """Device-level entry point on a caller stream equals the host path."""
+    torch = pytest.importorskip("torch")
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=14, n_models=64, steps=50)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        _, raw_ref, _ = ev.evaluate_batch(batch)
+        pk = ev.pack(batch)
+        me = torch.full((64,), 1000.0, dtype=torch.float64, device="cuda")
+        raw = torch.zeros(64, dtype=torch.float64, device="cuda")
+        steps = torch.zeros(64, dtype=torch.int32, device="cuda")
+        s = torch.cuda.current_stream()
+        pk.run(me.data_ptr(), raw.data_ptr(), steps.data_ptr(), s.cuda_stream)
+        s.synchronize()
+        assert np.array_equal(raw.cpu().numpy(), raw_ref)
+        assert (steps.cpu().numpy() == 50).all()
+        assert pk.info["n_models"] == 64
+        pk.free()
+
+
+def test_full_headline_workload_properties():
+    """All 4096 models x 2000 steps of the headline workload: deterministic
+    across runs, finite, every step run (min_conc_change 0), and a sample
+    agrees with the oracle."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=0)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        err1, raw1, st1 = ev.evaluate_batch(batch)
+        err2, raw2, st2 = ev.evaluate_batch(batch)
+    assert np.array_equal(raw1, raw2)
+    assert np.isfinite(raw1).all()
+    assert st1["cell_updates"] == 4096 * 2000 * 64 * 64
+    idx = np.arange(0, 4096, 512)
+    sub = batch.subset(idx)
+    oe, oraw, _ = oracle.evaluate_batch(params, init, tgt, sub)
+    assert_raw_close(raw1[idx], oraw, what="headline sample")
