@@ -227,7 +227,11 @@ def main():
     raw = torch.zeros(n, dtype=torch.float64, device="cuda")
     steps_out = torch.zeros(n, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the kernel, the flush and the events all run on it
+    # (the legacy default stream's handle is 0, which the C ABI reads as
+    # "the context's own stream").
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     def launch():
         pk.run(me.data_ptr(), raw.data_ptr(), steps_out.data_ptr(), stream.cuda_stream)

@@ -34,6 +34,10 @@ constexpr int kConstSlot = 255;
 
 // Header flags.
 constexpr uint32_t kFlagNone = 0u;
+// Every link has a finite K > 0 and a finite Hill coefficient and every gene
+// finite rates: on a non-negative finite state no link term can be NaN, so
+// the kernel may combine terms with min/max (see the kernel's regulation).
+constexpr uint32_t kFlagFast = 1u;
 
 struct alignas(16) PackedHeader {
   int32_t orig_index;  // position of the model in the caller's batch

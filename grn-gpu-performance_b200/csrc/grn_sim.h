@@ -24,7 +24,9 @@ struct SimArgs {
   int32_t Wg;                // float4 groups per row = ceil(W / 4)
   int32_t n_steps;           // max Euler steps per experiment
   int32_t fitness_kind;      // grn_fitness_kind
-  int32_t planes;            // state planes available per CTA
+  int32_t planes;            // shared-memory state planes per block (even)
+  int32_t fast_ok;           // experiments allow the fast path (non-negative
+                             // finite initial state, minConc >= 0)
   float dt;
   float min_conc;
   double min_conc_change;
@@ -36,7 +38,7 @@ struct SimArgs {
   int32_t *steps;            // [caller index] out, may be null
   int32_t *work_counter;     // zeroed before the launch
   int32_t *error_flag;       // set non-zero on an internal error
-  float *gstate;             // global state slots (GLOBAL schedule)
+  float *gstate;             // global state slots, one per block (or null)
   int64_t slot_floats;       // floats per global state slot
   float *state_out;          // optional final states
                              // [caller index][n_exp][state_planes][H][W]
@@ -45,22 +47,29 @@ struct SimArgs {
 
 // One compiled kernel variant.
 struct KernelVariant {
-  int schedule;     // grn_schedule (SMEM_1BUF / SMEM_2BUF share a kernel)
-  int threads;      // threads per block
-  int gmax;         // most genes a model may have
-  int items;        // float4 groups per thread when genes sit in registers
-  int nreg;         // most genes whose new values wait in registers
-  bool global_state;
+  int threads;  // threads per block
+  int gmax;     // most genes a model may have
+  int items;    // float4 groups each thread owns (fixed items)
+  bool loop;    // threads walk the grid's groups (any grid size)
+  bool ragged;  // compiled for W not a multiple of 4
 };
 
 // Launch plan chosen by the host.
 struct LaunchPlan {
   KernelVariant v;
+  int schedule;          // grn_schedule actually used
   int blocks;            // persistent grid size
-  int planes;            // state planes in shared memory (0 for GLOBAL)
+  int planes;            // state planes in shared memory (even; may be 0)
   size_t smem_bytes;     // dynamic shared memory
   int blocks_per_sm;
+  int64_t slot_floats;   // floats of one block's global state slot (0: none)
 };
+
+// Floats of one state plane of a W x H grid: rows padded to float4 groups,
+// plus a zero row above and below (see the kernel's Geom).
+inline int64_t plane_floats(int W, int H) {
+  return (int64_t)(H + 2) * 4 * ((W + 3) / 4);
+}
 
 // Bytes of shared memory a block needs besides the state planes.
 size_t sim_fixed_smem_bytes();

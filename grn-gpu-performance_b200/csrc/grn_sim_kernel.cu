@@ -74,228 +74,259 @@ constexpr size_t kStateOffset = (kWorkOffset + 16 + 127) & ~size_t(127);
 
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
 
-// Regulator lg2 values of one float4 group for a runtime slot.  The slot is
-// the same for every thread of the block, so the switch is a uniform branch.
-template <int GMAX>
-__device__ __forceinline__ float4 pick_slot(const float4 (&lg)[GMAX], int slot) {
-#define GRN_CASE(k)                       \
-  case k:                                 \
-    if constexpr (GMAX > k) return lg[k]; \
+// ---- regulation ------------------------------------------------------
+//
+// A gene's regulation is 1 / (1 + 2^V), V combined in exponent space over
+// its links (grn_packed.h).  Two combine modes:
+//   fast   min / max (fminf / fmaxf).  Identical to the reference whenever
+//          no link term is NaN, which the host guarantees for models with
+//          finite K > 0 and finite Hill coefficients on non-negative finite
+//          states (flag kFlagFast).
+//   exact  the reference's comparison order (simopor.cpp:20-22,
+//          simopand.cpp:20-22 with MathAlgo::max/min): a NaN term on
+//          either side yields the new term; a NaN start makes the first
+//          link's term the initial value ("first used link writes
+//          ratios[p]", modelsimulator.cpp:156-192).
+
+// Reference OR (Hill max) in exponent space: keep the running v only if it
+// is strictly smaller.
+__device__ __forceinline__ float comb_or(float run, float t) { return (run < t) ? run : t; }
+// Reference AND (Hill min) in exponent space.
+__device__ __forceinline__ float comb_and(float run, float t) { return (run > t) ? run : t; }
+
+enum CombMode { kOrFast, kAndFast, kOrExact, kAndExact };
+
+template <int MODE>
+__device__ __forceinline__ float comb(float run, float t) {
+  if constexpr (MODE == kOrFast) return fminf(run, t);
+  else if constexpr (MODE == kAndFast) return fmaxf(run, t);
+  else if constexpr (MODE == kOrExact) return comb_or(run, t);
+  else return comb_and(run, t);
+}
+
+template <int MODE>
+__device__ __forceinline__ void comb4(float4 &v, float a, const float4 &x, float b) {
+  v.x = comb<MODE>(v.x, fmaf(a, x.x, b));
+  v.y = comb<MODE>(v.y, fmaf(a, x.y, b));
+  v.z = comb<MODE>(v.z, fmaf(a, x.z, b));
+  v.w = comb<MODE>(v.w, fmaf(a, x.w, b));
+}
+
+// Applies one link to the running exponents of NI groups.  The regulator
+// slot is the same for every thread of the block; each case carries the
+// link's whole work so that the switch stays a (uniform) branch rather than
+// a select chain over all registers.
+template <int NI, int GMAX, int MODE>
+__device__ __forceinline__ void apply_link(float4 (&v)[NI], const PackedLink &lk,
+                                           const float4 (&lg)[NI][GMAX]) {
+#define GRN_CASE(k)                                                   \
+  case k:                                                             \
+    if constexpr (GMAX > k) {                                         \
+      _Pragma("unroll") for (int i = 0; i < NI; ++i)                  \
+          comb4<MODE>(v[i], lk.a, lg[i][k], lk.b);                    \
+    }                                                                 \
     break;
-  switch (slot) {
+  switch (lk.slot) {
     GRN_CASE(0) GRN_CASE(1) GRN_CASE(2) GRN_CASE(3)
     GRN_CASE(4) GRN_CASE(5) GRN_CASE(6) GRN_CASE(7)
     GRN_CASE(8) GRN_CASE(9) GRN_CASE(10) GRN_CASE(11)
     GRN_CASE(12) GRN_CASE(13) GRN_CASE(14) GRN_CASE(15)
-    default: break;
+    default:  // kConstSlot: lg2 value 0, a = b = 0 (Hill coefficient 0)
+#pragma unroll
+      for (int i = 0; i < NI; ++i) comb4<MODE>(v[i], lk.a, f4(0.0f), lk.b);
+      break;
   }
 #undef GRN_CASE
-  return f4(0.0f);  // kConstSlot: lg2 value 0 (Hill coefficient 0)
 }
 
-// Reference OR (Hill max, simopor.cpp:20-22 with MathAlgo::max) in exponent
-// space: keep the running v only if it is strictly smaller; a NaN on either
-// side yields the new term, as the reference's comparison does.
-__device__ __forceinline__ float comb_or(float run, float t) { return (run < t) ? run : t; }
-// Reference AND (Hill min, simopand.cpp:20-22 with MathAlgo::min).
-__device__ __forceinline__ float comb_and(float run, float t) { return (run > t) ? run : t; }
-
-// Regulation value of gene p for one float4 group: the result of the
-// reference's op list for the product (modelsimulator.cpp:156-192).
-template <int GMAX>
-__device__ __forceinline__ float4 regulation(const ModelSmem &M, int p,
-                                             const float4 (&lg)[GMAX]) {
-  const PackedGene &g = M.genes[p];
-  const int n_or = g.n_or, n_and = g.n_and;
-  if (n_or + n_and == 0) return f4(0.0f);  // OpZero
-  const float qnan = __int_as_float(0x7fc00000);
-  // A NaN start makes the first link's term the initial value, which is the
-  // reference's "first used link writes ratios[p]".
-  float4 v = f4(qnan);
-  const PackedLink *L = M.links + g.link_begin;
-  for (int l = 0; l < n_or; ++l) {
-    const PackedLink lk = L[l];
-    const float4 x = pick_slot<GMAX>(lg, lk.slot);
-    v.x = comb_or(v.x, fmaf(lk.a, x.x, lk.b));
-    v.y = comb_or(v.y, fmaf(lk.a, x.y, lk.b));
-    v.z = comb_or(v.z, fmaf(lk.a, x.z, lk.b));
-    v.w = comb_or(v.w, fmaf(lk.a, x.w, lk.b));
-  }
-  for (int l = n_or; l < n_or + n_and; ++l) {
-    const PackedLink lk = L[l];
-    const float4 x = pick_slot<GMAX>(lg, lk.slot);
-    v.x = comb_and(v.x, fmaf(lk.a, x.x, lk.b));
-    v.y = comb_and(v.y, fmaf(lk.a, x.y, lk.b));
-    v.z = comb_and(v.z, fmaf(lk.a, x.z, lk.b));
-    v.w = comb_and(v.w, fmaf(lk.a, x.w, lk.b));
-  }
-  float4 h;
-  h.x = rcp_approx(1.0f + ex2_approx(v.x));
-  h.y = rcp_approx(1.0f + ex2_approx(v.y));
-  h.z = rcp_approx(1.0f + ex2_approx(v.z));
-  h.w = rcp_approx(1.0f + ex2_approx(v.w));
-  return h;
-}
-
-// Rate, diffusion and Euler update of one cell
-// (modelsimulator.cpp:224-275).  A missing neighbour is passed as +0.0,
-// which leaves the reference's running sum unchanged.
-__device__ __forceinline__ float update_cell(float c, float h, float lim,
-                                             float deg, float dif, float left,
-                                             float right, float up, float down,
-                                             float tot, float dt,
-                                             float min_conc, bool valid,
-                                             float &mx) {
-  float r = fmaf(lim, h, -deg * c);
-  if (dif > 0.0f) {
-    const float s = ((left + right) + up) + down;
-    if (s > 0.0f || (tot > 0.0f && c > 0.0f)) r = fmaf(dif, fmaf(-tot, c, s), r);
-  }
-  float nc = c;
-  if (r != 0.0f) {  // NaN counts as non-zero, like the reference's `if (ratio)`
-    nc = fmaf(dt, r, c);
-    nc = (nc < min_conc) ? 0.0f : nc;
-    const float ar = fabsf(r);
-    if (valid) mx = (ar > mx) ? ar : mx;  // a NaN rate never raises the max
-  }
-  return valid ? nc : 0.0f;
-}
-
-// Geometry of the state: W x H cells, rows padded to Wp = 4 * Wg floats,
-// planes of P = H * Wp floats, Q = H * Wg float4 groups per plane.
-struct Geom {
-  int W, H, Wg, Wp, P, Q;
-};
-
-struct GroupPos {
-  int q;       // group index, clamped into [0, Q)
-  int y, x0;   // row and first column
-  bool valid;  // the group exists (q < Q before clamping)
-};
-
-__device__ __forceinline__ GroupPos group_pos(int q, const Geom &g) {
-  GroupPos p;
-  p.valid = q < g.Q;
-  p.q = p.valid ? q : g.Q - 1;
-  p.y = p.q / g.Wg;
-  p.x0 = (p.q - p.y * g.Wg) * 4;
-  return p;
-}
-
-// Cell-position facts of one float4 group shared by all its genes.
-struct GroupCells {
-  bool v0, v1, v2, v3;       // cell exists (x < W and group valid)
-  bool has_up, has_dn;       // neighbour rows exist
-  bool has_l, has_r;         // neighbour groups exist in the row
-  bool r0, r1, r2;           // right neighbour of cells 0..2 exists
-  float t0, t1, t2, t3;      // number of existing neighbours per cell
-};
-
-__device__ __forceinline__ GroupCells group_cells(const GroupPos &gp, const Geom &g) {
-  GroupCells c;
-  const int W = g.W;
-  c.v0 = gp.valid && gp.x0 + 0 < W;
-  c.v1 = gp.valid && gp.x0 + 1 < W;
-  c.v2 = gp.valid && gp.x0 + 2 < W;
-  c.v3 = gp.valid && gp.x0 + 3 < W;
-  c.has_up = gp.y > 0;
-  c.has_dn = gp.y < g.H - 1;
-  c.has_l = gp.x0 > 0;
-  c.has_r = gp.x0 + 4 < W;
-  c.r0 = gp.x0 + 1 < W;
-  c.r1 = gp.x0 + 2 < W;
-  c.r2 = gp.x0 + 3 < W;
-  const float tv = (c.has_up ? 1.0f : 0.0f) + (c.has_dn ? 1.0f : 0.0f);
-  c.t0 = tv + (c.has_l ? 1.0f : 0.0f) + (c.r0 ? 1.0f : 0.0f);
-  c.t1 = tv + 1.0f + (c.r1 ? 1.0f : 0.0f);
-  c.t2 = tv + 1.0f + (c.r2 ? 1.0f : 0.0f);
-  c.t3 = tv + 1.0f + (c.has_r ? 1.0f : 0.0f);
-  return c;
-}
-
-// lg2 of the current value of every regulator gene of one group.
-template <int GMAX>
-__device__ __forceinline__ void group_lg(const ModelSmem &M, const float *st,
-                                         int plane_shift_planes, int n_dbuf,
-                                         const Geom &g, int base,
-                                         float4 (&lg)[GMAX]) {
-  const int G = M.hdr.n_genes;
-  const uint32_t lg_mask = M.hdr.lg_mask;
+// Regulation of one gene for NI groups.
+template <int NI, int GMAX, bool EXACT>
+__device__ __forceinline__ void regulation(const ModelSmem &M, const PackedGene &g,
+                                           const float4 (&lg)[NI][GMAX], float4 (&h)[NI]) {
+  const int n_or = g.n_or, n = g.n_or + g.n_and;
+  if (n == 0) {  // OpZero
 #pragma unroll
-  for (int k = 0; k < GMAX; ++k) {
-    lg[k] = f4(0.0f);
-    if (k < G && ((lg_mask >> k) & 1u)) {
-      const int plane = (k < n_dbuf) ? k + plane_shift_planes : k;
-      const float4 c = *reinterpret_cast<const float4 *>(st + plane * g.P + base);
-      lg[k].x = lg2_approx(c.x);
-      lg[k].y = lg2_approx(c.y);
-      lg[k].z = lg2_approx(c.z);
-      lg[k].w = lg2_approx(c.w);
-    }
+    for (int i = 0; i < NI; ++i) h[i] = f4(0.0f);
+    return;
+  }
+  float4 v[NI];
+  // exact: a NaN start makes the first term the initial value; fast: min
+  // over OR terms, then max with each AND term.
+  const float v0 = EXACT ? __int_as_float(0x7fc00000)
+                         : (n_or > 0 ? __int_as_float(0x7f800000) : __int_as_float(0xff800000));
+#pragma unroll
+  for (int i = 0; i < NI; ++i) v[i] = f4(v0);
+  const PackedLink *L = M.links + g.link_begin;
+  int l = 0;
+  for (; l < n_or; ++l) apply_link<NI, GMAX, EXACT ? kOrExact : kOrFast>(v, L[l], lg);
+  for (; l < n; ++l) apply_link<NI, GMAX, EXACT ? kAndExact : kAndFast>(v, L[l], lg);
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    h[i].x = rcp_approx(1.0f + ex2_approx(v[i].x));
+    h[i].y = rcp_approx(1.0f + ex2_approx(v[i].y));
+    h[i].z = rcp_approx(1.0f + ex2_approx(v[i].z));
+    h[i].w = rcp_approx(1.0f + ex2_approx(v[i].w));
   }
 }
 
-// New value of gene p for one float4 group whose current plane is `pl`.
-// All lanes of a warp call this together (it shuffles).  Updates mx with the
-// max |rate| over valid cells.
-template <int GMAX>
-__device__ __forceinline__ float4 gene_update(const ModelSmem &M, int p,
-                                              const float4 (&lg)[GMAX],
-                                              const float *pl, const Geom &g,
-                                              const GroupPos &gp,
-                                              const GroupCells &cc, int lane,
-                                              float dt, float min_conc,
-                                              float &mx) {
-  const float4 h = regulation<GMAX>(M, p, lg);
-  const PackedGene &gn = M.genes[p];
-  const float lim = gn.lim, deg = gn.deg, dif = gn.dif;
-  const int base = gp.q * 4;
-  const float4 c = *reinterpret_cast<const float4 *>(pl + base);
-  float4 up = f4(0.0f), dn = f4(0.0f);
-  float lft = 0.0f, rgt = 0.0f;
-  if (dif > 0.0f) {  // uniform: the same gene for the whole block
-    if (cc.has_up) up = *reinterpret_cast<const float4 *>(pl + base - g.Wp);
-    if (cc.has_dn) dn = *reinterpret_cast<const float4 *>(pl + base + g.Wp);
-    lft = __shfl_up_sync(kFull, c.w, 1);
-    rgt = __shfl_down_sync(kFull, c.x, 1);
-    // Lanes 0 and 31 have no in-warp neighbour group.
-    if (lane == 0 && cc.has_l) lft = pl[base - 1];
-    if (lane == 31 && cc.has_r) rgt = pl[base + 4];
-    if (!cc.has_l) lft = 0.0f;
-    if (!cc.has_r) rgt = 0.0f;
+// ---- geometry ----------------------------------------------------------
+//
+// A state plane holds the W x H grid as rows of RS = 4 * Wg floats (rows
+// padded to whole float4 groups) plus one zero row above and one below:
+// PS = (H + 2) * RS floats, row y at (y + 1) * RS.  The zero rows make the
+// up/down neighbours of the first and last rows read +0.0, which leaves the
+// reference's neighbour sum unchanged.  Steps write data groups only; when W
+// is not a multiple of 4 the cells past W of a row's last group are written
+// as 0 and serve as that row's right border.
+struct Geom {
+  int W, H, Wg, RS, PS, Q;
+};
+
+// One float4 group a thread owns, with everything a step needs about its
+// position (computed once per launch for fixed items).
+struct Item {
+  int base;           // float offset of the group in a plane
+  float4 tot;         // existing neighbours of each cell (reference `total`)
+  bool valid;         // the group exists (an index past the end is clamped
+                      // onto the last group so the lane still shuffles)
+  bool lfix, rfix;    // the neighbour group lives in another warp: read it
+  bool lzero, rzero;  // no neighbour group (grid border)
+  bool v1, v2, v3;    // cells 1..3 of the group exist (cell 0 always does)
+};
+
+__device__ __forceinline__ Item make_item(int y, int gx, bool valid, int lane,
+                                          const Geom &g) {
+  Item it;
+  it.valid = valid;
+  it.base = (y + 1) * g.RS + 4 * gx;
+  const int x0 = 4 * gx;
+  const float tv = (y > 0 ? 1.0f : 0.0f) + (y < g.H - 1 ? 1.0f : 0.0f);
+  it.tot.x = tv + (x0 > 0 ? 1.0f : 0.0f) + (x0 + 1 < g.W ? 1.0f : 0.0f);
+  it.tot.y = tv + 1.0f + (x0 + 2 < g.W ? 1.0f : 0.0f);
+  it.tot.z = tv + 1.0f + (x0 + 3 < g.W ? 1.0f : 0.0f);
+  it.tot.w = tv + 1.0f + (x0 + 4 < g.W ? 1.0f : 0.0f);
+  it.lzero = gx == 0;
+  it.rzero = gx == g.Wg - 1;
+  it.lfix = lane == 0 && !it.lzero;
+  it.rfix = lane == 31 && !it.rzero;
+  it.v1 = x0 + 1 < g.W;
+  it.v2 = x0 + 2 < g.W;
+  it.v3 = x0 + 3 < g.W;
+  return it;
+}
+
+__device__ __forceinline__ Item item_at(int q, int lane, const Geom &g) {
+  const bool valid = q < g.Q;
+  const int qc = valid ? q : g.Q - 1;
+  const int y = qc / g.Wg;
+  return make_item(y, qc - y * g.Wg, valid, lane, g);
+}
+
+__device__ __forceinline__ int cell_offset(const Geom &g, int y, int x) {
+  return (y + 1) * g.RS + x;
+}
+
+// Euler update of one cell (modelsimulator.cpp:224-275).
+//   r = lim*h - deg*c (+ dif*(s - tot*c) for diffusing genes)
+// exact: the reference's guard on the diffusion term, "a zero rate keeps
+// the value", the minConc clamp and a NaN-ignoring max.
+// fast (minConc 0 and a non-negative finite state, host-checked): the guard
+// only ever skips adding dif*0, a zero rate gives c + dt*0 = c, and the
+// clamp is a max with 0, so these simplify without changing any result.
+template <bool EXACT>
+__device__ __forceinline__ float update_cell(float c, float h, float lim, float deg,
+                                             float dif, bool diffuses, float s, float tot,
+                                             float dt, float min_conc, float &mx) {
+  float r = fmaf(-deg, c, lim * h);
+  if constexpr (EXACT) {
+    if (diffuses && (s > 0.0f || (tot > 0.0f && c > 0.0f))) r = fmaf(dif, fmaf(-tot, c, s), r);
+    float nc = c;
+    if (r != 0.0f) {  // NaN counts as non-zero, like the reference's `if (ratio)`
+      nc = fmaf(dt, r, c);
+      nc = (nc < min_conc) ? 0.0f : nc;
+      const float ar = fabsf(r);
+      mx = (ar > mx) ? ar : mx;  // a NaN rate never raises the max
+    }
+    return nc;
+  } else {
+    if (diffuses) r = fmaf(dif, fmaf(-tot, c, s), r);
+    mx = fmaxf(mx, fabsf(r));
+    return fmaxf(fmaf(dt, r, c), 0.0f);
   }
-  float4 nv;
-  nv.x = update_cell(c.x, h.x, lim, deg, dif, lft, cc.r0 ? c.y : 0.0f, up.x,
-                     dn.x, cc.t0, dt, min_conc, cc.v0, mx);
-  nv.y = update_cell(c.y, h.y, lim, deg, dif, c.x, cc.r1 ? c.z : 0.0f, up.y,
-                     dn.y, cc.t1, dt, min_conc, cc.v1, mx);
-  nv.z = update_cell(c.z, h.z, lim, deg, dif, c.y, cc.r2 ? c.w : 0.0f, up.z,
-                     dn.z, cc.t2, dt, min_conc, cc.v2, mx);
-  nv.w = update_cell(c.w, h.w, lim, deg, dif, c.z, rgt, up.w, dn.w, cc.t3, dt,
-                     min_conc, cc.v3, mx);
-  return nv;
+}
+
+// New values of one gene for NI groups; `cur` points at the gene's current
+// plane (shared or global memory).  All lanes of a warp call this together
+// (it shuffles).  `mx` takes the max |rate| of the valid groups' real cells.
+template <int NI, int GMAX, bool EXACT, bool RAGGED>
+__device__ __forceinline__ void gene_update(const ModelSmem &M, const PackedGene &gn,
+                                            const float4 (&lg)[NI][GMAX], const float *cur,
+                                            const Geom &g, const Item (&it)[NI], float dt,
+                                            float min_conc, float &mx, float4 (&nv)[NI]) {
+  float4 h[NI];
+  regulation<NI, GMAX, EXACT>(M, gn, lg, h);
+  const bool diffuses = gn.dif > 0.0f;  // uniform: the same gene for the whole block
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    const float4 c = *reinterpret_cast<const float4 *>(cur + it[i].base);
+    float4 s = f4(0.0f);
+    if (diffuses) {
+      const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
+      const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
+      float lft = __shfl_up_sync(kFull, c.w, 1);
+      float rgt = __shfl_down_sync(kFull, c.x, 1);
+      if (it[i].lfix) lft = cur[it[i].base - 1];
+      if (it[i].rfix) rgt = cur[it[i].base + 4];
+      if (it[i].lzero) lft = 0.0f;
+      if (it[i].rzero) rgt = 0.0f;
+      // Reference order: x-1, x+1, y-1, y+1.
+      s.x = ((lft + c.y) + up.x) + dn.x;
+      s.y = ((c.x + c.z) + up.y) + dn.y;
+      s.z = ((c.y + c.w) + up.z) + dn.z;
+      s.w = ((c.z + rgt) + up.w) + dn.w;
+    }
+    float m = 0.0f, m1 = 0.0f, m2 = 0.0f, m3 = 0.0f;
+    nv[i].x = update_cell<EXACT>(c.x, h[i].x, gn.lim, gn.deg, gn.dif, diffuses, s.x,
+                                 it[i].tot.x, dt, min_conc, m);
+    nv[i].y = update_cell<EXACT>(c.y, h[i].y, gn.lim, gn.deg, gn.dif, diffuses, s.y,
+                                 it[i].tot.y, dt, min_conc, RAGGED ? m1 : m);
+    nv[i].z = update_cell<EXACT>(c.z, h[i].z, gn.lim, gn.deg, gn.dif, diffuses, s.z,
+                                 it[i].tot.z, dt, min_conc, RAGGED ? m2 : m);
+    nv[i].w = update_cell<EXACT>(c.w, h[i].w, gn.lim, gn.deg, gn.dif, diffuses, s.w,
+                                 it[i].tot.w, dt, min_conc, RAGGED ? m3 : m);
+    if constexpr (RAGGED) {
+      // Cells past W are padding: kept at 0, never part of the max.
+      if (!it[i].v1) { nv[i].y = 0.0f; m1 = 0.0f; }
+      if (!it[i].v2) { nv[i].z = 0.0f; m2 = 0.0f; }
+      if (!it[i].v3) { nv[i].w = 0.0f; m3 = 0.0f; }
+      m = fmaxf(fmaxf(m, m1), fmaxf(m2, m3));
+    }
+    if (it[i].valid) mx = fmaxf(mx, m);
+  }
 }
 
 // Block-wide max of a non-negative, non-NaN float (bit order == value
 // order).  `parity` alternates two buffers so that one barrier per step
 // suffices.
 template <int NT>
-__device__ __forceinline__ float block_max(float v, float *red, int parity,
-                                           int lane, int warp) {
+__device__ __forceinline__ float block_max(float v, float *red, int parity, int lane,
+                                           int warp) {
   const unsigned bits = __reduce_max_sync(kFull, __float_as_uint(v));
   float *r = red + parity * 32;
   if (lane == 0) r[warp] = __uint_as_float(bits);
   __syncthreads();
-  float m = r[0];
+  float m = 0.0f;
 #pragma unroll
-  for (int w = 1; w < NT / 32; ++w) m = fmaxf(m, r[w]);
+  for (int w = 0; w < NT / 32; w += 4) {
+    const float4 v4 = *reinterpret_cast<const float4 *>(r + w);
+    m = fmaxf(m, fmaxf(fmaxf(v4.x, v4.y), fmaxf(v4.z, v4.w)));
+  }
   return m;
 }
 
 // Block-wide FP64 sum; every thread gets the same value (fixed order).
 template <int NT>
-__device__ __forceinline__ double block_sum(double v, double *dred, int lane,
-                                            int warp) {
+__device__ __forceinline__ double block_sum(double v, double *dred, int lane, int warp) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
   if (lane == 0) dred[warp] = v;
@@ -306,43 +337,113 @@ __device__ __forceinline__ double block_sum(double v, double *dred, int lane,
   return s;
 }
 
+// Where a model's state lives during one step: genes p < n_sm are double
+// buffered in shared-memory planes p and p + n_sm; the others in the
+// block's global slot, planes p and p + GMAX.  `par` selects the buffer
+// holding the current values.
+struct StatePtrs {
+  float *sm;   // shared-memory planes
+  float *gl;   // global-memory slot
+  int n_sm;    // genes held in shared memory
+};
+
+template <int GMAX>
+__device__ __forceinline__ float *plane_of(const StatePtrs &sp, const Geom &g, int p, int par) {
+  return p < sp.n_sm ? sp.sm + (p + (par ? sp.n_sm : 0)) * g.PS
+                     : sp.gl + (p + (par ? GMAX : 0)) * g.PS;
+}
+
+// New values of all genes of NI groups: shared-memory genes first, then
+// global-memory genes (two loops so that each uses its own load path).
+template <int NI, int GMAX, bool EXACT, bool RAGGED>
+__device__ __forceinline__ void group_step(const ModelSmem &M, const StatePtrs &sp,
+                                           const Geom &g, const Item (&it)[NI], int par,
+                                           float dt, float min_conc, float &mx) {
+  const int G = M.hdr.n_genes;
+  const uint32_t lg_mask = M.hdr.lg_mask;
+  const float *sm_cur = sp.sm + (par ? sp.n_sm : 0) * g.PS;
+  float *sm_nxt = sp.sm + (par ? 0 : sp.n_sm) * g.PS;
+  const float *gl_cur = sp.gl + (par ? GMAX : 0) * g.PS;
+  float *gl_nxt = sp.gl + (par ? 0 : GMAX) * g.PS;
+  // lg2 of every regulator gene's current value (0 for genes no link reads).
+  float4 lg[NI][GMAX];
+#pragma unroll
+  for (int k = 0; k < GMAX; ++k) {
+#pragma unroll
+    for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
+    if (k < G && ((lg_mask >> k) & 1u)) {
+      const float *pl = (k < sp.n_sm ? sm_cur : gl_cur) + k * g.PS;
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        const float4 c = *reinterpret_cast<const float4 *>(pl + it[i].base);
+        lg[i][k].x = lg2_approx(c.x);
+        lg[i][k].y = lg2_approx(c.y);
+        lg[i][k].z = lg2_approx(c.z);
+        lg[i][k].w = lg2_approx(c.w);
+      }
+    }
+  }
+  for (int p = 0; p < sp.n_sm; ++p) {
+    const PackedGene gn = M.genes[p];
+    float4 nv[NI];
+    gene_update<NI, GMAX, EXACT, RAGGED>(M, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc, mx,
+                                         nv);
+#pragma unroll
+    for (int i = 0; i < NI; ++i)
+      if (it[i].valid) *reinterpret_cast<float4 *>(sm_nxt + p * g.PS + it[i].base) = nv[i];
+  }
+  for (int p = sp.n_sm; p < G; ++p) {
+    const PackedGene gn = M.genes[p];
+    float4 nv[NI];
+    gene_update<NI, GMAX, EXACT, RAGGED>(M, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc, mx,
+                                         nv);
+#pragma unroll
+    for (int i = 0; i < NI; ++i)
+      if (it[i].valid) *reinterpret_cast<float4 *>(gl_nxt + p * g.PS + it[i].base) = nv[i];
+  }
+}
+
 // The simulation kernel.
-//   NT     threads per block
-//   GMAX   most genes (products in use) per model
-//   ITEMS  float4 groups per thread when genes are held in registers
-//   NREG   most genes whose new values are held in registers across the
-//          barrier (the others are double buffered in spare planes)
-//   GSTATE state in global-memory slots instead of shared memory
-//
-// State planes: genes 0..G-1 start in planes 0..G-1.  With S = planes - G
-// spare planes, genes p < min(S, G) are double buffered: their current
-// plane is p on even steps and G + p on odd steps.  Genes p >= S keep plane
-// p and their new values wait in registers until all reads are done.
-template <int NT, int GMAX, int ITEMS, int NREG, bool GSTATE>
-__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2))
-    sim_kernel(const SimArgs A) {
+//   NT      threads per block
+//   GMAX    most genes (products in use) per model
+//   ITEMS   float4 groups each thread owns when LOOP is false (geometry
+//           computed once per launch)
+//   LOOP    grids with more groups than NT * ITEMS: each thread walks its
+//           groups with incrementally updated geometry
+//   RAGGED  W is not a multiple of 4
+template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED>
+__global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
   float *s_red = reinterpret_cast<float *>(smem + kRedOffset);
   double *s_dred = reinterpret_cast<double *>(smem + kDredOffset);
   int *s_work = reinterpret_cast<int *>(smem + kWorkOffset);
-  float *state;
-  if constexpr (GSTATE)
-    state = A.gstate + (size_t)blockIdx.x * (size_t)A.slot_floats;
-  else
-    state = reinterpret_cast<float *>(smem + kStateOffset);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   Geom g;
   g.W = A.W;
   g.H = A.H;
   g.Wg = A.Wg;
-  g.Wp = A.Wg * 4;
-  g.P = A.H * g.Wp;
+  g.RS = 4 * A.Wg;
+  g.PS = (A.H + 2) * g.RS;
   g.Q = A.H * A.Wg;
-  const int n_iter = (g.Q + NT - 1) / NT;  // same for every thread
   const float dt = A.dt, min_conc = A.min_conc;
   uint4 *Mw = reinterpret_cast<uint4 *>(smem);
+
+  StatePtrs sp;
+  sp.sm = reinterpret_cast<float *>(smem + kStateOffset);
+  sp.gl = A.gstate ? A.gstate + (size_t)blockIdx.x * (size_t)A.slot_floats : nullptr;
+
+  // Fixed items: geometry once per launch.
+  Item items[LOOP ? 1 : ITEMS];
+  if constexpr (!LOOP) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) items[i] = item_at(tid + i * NT, lane, g);
+  }
+  // Walking items: start and per-iteration stride of (row, group column).
+  const int y0 = tid / g.Wg, gx0 = tid - y0 * g.Wg;
+  const int dy = NT / g.Wg, dgx = NT - dy * g.Wg;
+  const int n_iter = (g.Q + NT - 1) / NT;
 
   for (;;) {
     if (tid == 0) *s_work = atomicAdd(A.work_counter, 1);
@@ -364,12 +465,11 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2))
     __syncthreads();
     const int G = M.hdr.n_genes;
     const int orig = M.hdr.orig_index;
-    const int S = GSTATE ? G : max(0, A.planes - G);  // spare planes
-    const int n_dbuf = min(S, G);                       // double-buffered genes
-    const int n_reg = G - n_dbuf;                       // register-held genes
-    bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
-               M.hdr.n_links > GRN_MAX_LINKS || n_reg > NREG ||
-               (n_reg > 0 && n_iter > ITEMS) || (!GSTATE && G > A.planes);
+    sp.n_sm = min(G, A.planes / 2);
+    const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast));
+    const bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
+                     M.hdr.n_links > GRN_MAX_LINKS || (sp.n_sm < G && sp.gl == nullptr) ||
+                     (!LOOP && n_iter > ITEMS);
     if (bad) {
       if (tid == 0) {
         atomicExch(A.error_flag, 1);
@@ -385,119 +485,82 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2))
     const double max_err = A.max_error[orig];
 
     for (int e = 0; e < A.n_exp && error <= max_err; ++e) {
-      // Initial state: input morphogen planes from the experiment, the
-      // other products 0 (simstate.cpp:64-90).  Padding cells are 0.
+      // Initial state, both buffers of every gene: input morphogen planes
+      // from the experiment, the other products 0 (simstate.cpp:64-90);
+      // zero rows and padding cells 0.
       const float *init = A.initial + (size_t)e * A.n_in * A.W * A.H;
-      for (int i = tid; i < G * g.P; i += NT) {
-        const int k = i / g.P, r = i - k * g.P;
-        const int y = r / g.Wp, x = r - y * g.Wp;
+      for (int i = tid; i < 2 * G * g.PS; i += NT) {
+        const int kb = i / g.PS, r = i - kb * g.PS;
+        const int kk = kb < G ? kb : kb - G;  // gene of this plane
+        const int y = r / g.RS - 1, x = r - (y + 1) * g.RS;
         float v = 0.0f;
-        if (k < A.n_in && x < g.W) v = init[((size_t)k * g.H + y) * g.W + x];
-        state[i] = v;
+        if (kb < G && kk < A.n_in && y >= 0 && y < g.H && x < g.W)
+          v = init[((size_t)kk * g.H + y) * g.W + x];
+        float *pl = plane_of<GMAX>(sp, g, kk, kb < G ? 0 : 1);
+        pl[r] = v;
       }
       __syncthreads();
 
       double change = 1.0;
       int step = 0;
-      int parity = 0;  // double-buffered genes live in planes G.. on odd steps
+      int par = 0;  // buffer holding the current values
       while (step < A.n_steps && change > A.min_conc_change) {
-        const int cur_shift = parity ? G : 0;   // plane offset of current values
-        const int nxt_shift = parity ? 0 : G;   // plane offset of next values
         float mx = 0.0f;
-        if constexpr (NREG == 0) {
-          for (int it = 0; it < n_iter; ++it) {
-            const GroupPos gp = group_pos(tid + it * NT, g);
-            const GroupCells cc = group_cells(gp, g);
-            float4 lg[GMAX];
-            group_lg<GMAX>(M, state, cur_shift, n_dbuf, g, gp.q * 4, lg);
-            for (int p = 0; p < G; ++p) {
-              const float4 nv = gene_update<GMAX>(M, p, lg, state + (p + cur_shift) * g.P,
-                                                  g, gp, cc, lane, dt, min_conc, mx);
-              if (gp.valid)
-                *reinterpret_cast<float4 *>(state + (p + nxt_shift) * g.P + gp.q * 4) = nv;
-            }
-          }
-          change = (double)block_max<NT>(mx, s_red, parity, lane, warp);
+        if constexpr (!LOOP) {
+          // All ITEMS groups of the thread at once (items past the grid are
+          // clamped duplicates and store nothing).
+          if (exact)
+            group_step<ITEMS, GMAX, true, RAGGED>(M, sp, g, items, par, dt, min_conc, mx);
+          else
+            group_step<ITEMS, GMAX, false, RAGGED>(M, sp, g, items, par, dt, min_conc, mx);
         } else {
-          float4 nreg[ITEMS][NREG];
-#pragma unroll
-          for (int it = 0; it < ITEMS; ++it) {
-            if (it < n_iter) {
-              const GroupPos gp = group_pos(tid + it * NT, g);
-              const GroupCells cc = group_cells(gp, g);
-              float4 lg[GMAX];
-              group_lg<GMAX>(M, state, cur_shift, n_dbuf, g, gp.q * 4, lg);
-              for (int p = 0; p < n_dbuf; ++p) {
-                const float4 nv = gene_update<GMAX>(M, p, lg, state + (p + cur_shift) * g.P,
-                                                    g, gp, cc, lane, dt, min_conc, mx);
-                if (gp.valid)
-                  *reinterpret_cast<float4 *>(state + (p + nxt_shift) * g.P + gp.q * 4) = nv;
-              }
-#pragma unroll
-              for (int r = 0; r < NREG; ++r) {
-                const int p = n_dbuf + r;
-                if (r < n_reg)
-                  nreg[it][r] = gene_update<GMAX>(M, p, lg, state + p * g.P, g, gp, cc,
-                                                  lane, dt, min_conc, mx);
-              }
+          int y = y0, gx = gx0;
+          for (int i = 0; i < n_iter; ++i) {
+            const int q = tid + i * NT;
+            const bool valid = q < g.Q;
+            const Item it[1] = {valid ? make_item(y, gx, true, lane, g) : item_at(q, lane, g)};
+            if (exact)
+              group_step<1, GMAX, true, RAGGED>(M, sp, g, it, par, dt, min_conc, mx);
+            else
+              group_step<1, GMAX, false, RAGGED>(M, sp, g, it, par, dt, min_conc, mx);
+            y += dy;
+            gx += dgx;
+            if (gx >= g.Wg) {
+              gx -= g.Wg;
+              ++y;
             }
-          }
-          change = (double)block_max<NT>(mx, s_red, parity, lane, warp);
-          if (n_reg > 0) {
-#pragma unroll
-            for (int it = 0; it < ITEMS; ++it) {
-              if (it < n_iter) {
-                const GroupPos gp = group_pos(tid + it * NT, g);
-                if (gp.valid) {
-#pragma unroll
-                  for (int r = 0; r < NREG; ++r)
-                    if (r < n_reg)
-                      *reinterpret_cast<float4 *>(state + (n_dbuf + r) * g.P + gp.q * 4) =
-                          nreg[it][r];
-                }
-              }
-            }
-            __syncthreads();
           }
         }
-        parity ^= 1;
+        change = (double)block_max<NT>(mx, s_red, par, lane, warp);
+        par ^= 1;
         ++step;
       }
       steps_total += step;
       change_sum += change;
       if (A.state_out) {
         // Final state of this experiment, unpadded [gene][y][x].
-        const int fin = parity ? G : 0;
         const int planes_out = min(G, A.state_planes);
         float *so = A.state_out + ((size_t)orig * A.n_exp + e) * A.state_planes * g.W * g.H;
         for (int i = tid; i < planes_out * g.W * g.H; i += NT) {
-          const int k = i / (g.W * g.H), r = i - k * g.W * g.H;
+          const int kk = i / (g.W * g.H), r = i - kk * g.W * g.H;
           const int y = r / g.W, x = r - y * g.W;
-          const int plane = k < n_dbuf ? k + fin : k;
-          so[i] = state[plane * g.P + y * g.Wp + x];
+          so[i] = plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
         }
       }
 
       // Fitness of the experiment (simstate.cpp:135-158), FP64 sums.
       const float *tgt = A.target + (size_t)e * A.n_target * A.W * A.H;
-      const int fin_shift = parity ? G : 0;
       double acc = 0.0;
-      for (int q = tid; q < g.Q; q += NT) {
-        const int y = q / g.Wg, x0 = (q - y * g.Wg) * 4;
-        for (int j = 0; j < 4; ++j) {
-          const int x = x0 + j;
-          if (x >= g.W) break;
-          for (int k = 0; k < A.n_target; ++k) {
-            const int gene = A.n_in + k;
-            const int plane = gene < n_dbuf ? gene + fin_shift : gene;
-            const double a = state[plane * g.P + q * 4 + j];
-            const double b = tgt[((size_t)k * g.H + y) * g.W + x];
-            if (A.fitness_kind == GRN_FITNESS_MSE) {
-              acc += (a - b) * (a - b);
-            } else {
-              const double sub = fabs(a - b) - A.dist_threshold;
-              if (sub > 0) acc += log(1.0 + sub);
-            }
+      for (int i = tid; i < g.W * g.H; i += NT) {
+        const int y = i / g.W, x = i - y * g.W;
+        for (int kk = 0; kk < A.n_target; ++kk) {
+          const double a = plane_of<GMAX>(sp, g, A.n_in + kk, par)[cell_offset(g, y, x)];
+          const double b = tgt[(size_t)kk * g.W * g.H + i];
+          if (A.fitness_kind == GRN_FITNESS_MSE) {
+            acc += (a - b) * (a - b);
+          } else {
+            const double sub = fabs(a - b) - A.dist_threshold;
+            if (sub > 0) acc += log(1.0 + sub);
           }
         }
       }
@@ -528,21 +591,16 @@ struct VariantEntry {
   KernelFn fn;
 };
 
-#define GRN_SMEM_VARIANT(NT, GMAX, ITEMS, NREG)            \
-  {{GRN_SCHEDULE_SMEM_1BUF, NT, GMAX, ITEMS, NREG, false}, \
-   &sim_kernel<NT, GMAX, ITEMS, NREG, false>}
-#define GRN_GLOBAL_VARIANT(NT, GMAX) \
-  {{GRN_SCHEDULE_GLOBAL, NT, GMAX, 1, 0, true}, &sim_kernel<NT, GMAX, 1, 0, true>}
+#define GRN_VARIANT(NT, GMAX, ITEMS, LOOP)                                          \
+  {{NT, GMAX, ITEMS, LOOP, false}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false>},       \
+  {{NT, GMAX, ITEMS, LOOP, true}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true>}
 
 const VariantEntry kVariants[] = {
-    GRN_SMEM_VARIANT(256, 4, 1, 0),   GRN_SMEM_VARIANT(256, 8, 1, 0),
-    GRN_SMEM_VARIANT(256, 16, 1, 0),  GRN_SMEM_VARIANT(512, 4, 1, 0),
-    GRN_SMEM_VARIANT(512, 8, 1, 0),   GRN_SMEM_VARIANT(512, 16, 1, 0),
-    GRN_SMEM_VARIANT(1024, 4, 1, 0),  GRN_SMEM_VARIANT(256, 8, 1, 4),
-    GRN_SMEM_VARIANT(512, 8, 2, 4),   GRN_SMEM_VARIANT(256, 4, 4, 4),
-    GRN_SMEM_VARIANT(512, 4, 2, 4),   GRN_SMEM_VARIANT(256, 16, 1, 8),
-    GRN_GLOBAL_VARIANT(256, 16),      GRN_GLOBAL_VARIANT(512, 8),
-    GRN_GLOBAL_VARIANT(512, 16),
+    GRN_VARIANT(256, 4, 1, false),  GRN_VARIANT(256, 8, 1, false),
+    GRN_VARIANT(256, 16, 1, false), GRN_VARIANT(512, 4, 2, false),
+    GRN_VARIANT(512, 8, 2, false),
+    GRN_VARIANT(512, 8, 1, true),   GRN_VARIANT(512, 16, 1, true),
+    GRN_VARIANT(256, 4, 1, true),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -550,7 +608,7 @@ const VariantEntry *find_variant(const KernelVariant &v) {
   for (int i = 0; i < kNumVariants; ++i) {
     const KernelVariant &k = kVariants[i].v;
     if (k.threads == v.threads && k.gmax == v.gmax && k.items == v.items &&
-        k.nreg == v.nreg && k.global_state == v.global_state)
+        k.loop == v.loop && k.ragged == v.ragged)
       return &kVariants[i];
   }
   return nullptr;
@@ -564,27 +622,25 @@ int sim_variant_count() { return kNumVariants; }
 
 KernelVariant sim_variant(int i) { return kVariants[i].v; }
 
-cudaError_t sim_occupancy(const KernelVariant &v, size_t smem_bytes,
-                          int *blocks_per_sm) {
+cudaError_t sim_occupancy(const KernelVariant &v, size_t smem_bytes, int *blocks_per_sm) {
   const VariantEntry *e = find_variant(v);
   if (!e) return cudaErrorInvalidValue;
-  cudaError_t err = cudaFuncSetAttribute(
-      e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  cudaError_t err =
+      cudaFuncSetAttribute(e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (err != cudaSuccess) {
     *blocks_per_sm = 0;
     cudaGetLastError();
     return cudaSuccess;
   }
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, e->fn,
-                                                       v.threads, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, e->fn, v.threads,
+                                                       smem_bytes);
 }
 
-cudaError_t sim_launch(const LaunchPlan &plan, const SimArgs &args,
-                       cudaStream_t stream) {
+cudaError_t sim_launch(const LaunchPlan &plan, const SimArgs &args, cudaStream_t stream) {
   const VariantEntry *e = find_variant(plan.v);
   if (!e) return cudaErrorInvalidValue;
-  cudaError_t err = cudaFuncSetAttribute(
-      e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem_bytes);
+  cudaError_t err = cudaFuncSetAttribute(e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)plan.smem_bytes);
   if (err != cudaSuccess) return err;
   e->fn<<<plan.blocks, plan.v.threads, plan.smem_bytes, stream>>>(args);
   return cudaGetLastError();

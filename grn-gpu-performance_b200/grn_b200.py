@@ -28,8 +28,8 @@ STATUS_NAMES = {0: "GRN_OK", 1: "GRN_ERR_INVALID_ARGUMENT", 2: "GRN_ERR_NO_DEVIC
                 9: "GRN_ERR_NOT_FOUND", 10: "GRN_ERR_KERNEL"}
 FITNESS_REF_LOGTHRESH = 0
 FITNESS_MSE = 1
-SCHEDULE_AUTO, SCHEDULE_SMEM_1BUF, SCHEDULE_SMEM_2BUF, SCHEDULE_GLOBAL = 0, 1, 2, 3
-SCHEDULE_NAMES = {0: "auto", 1: "smem_regs", 2: "smem_2buf", 3: "global"}
+SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1, 2, 3
+SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global"}
 
 
 class SimParams(ctypes.Structure):
@@ -324,11 +324,13 @@ class Packed:
         self.info = {name: getattr(info, name) for name, _ in PackedInfo._fields_}
 
     def run(self, d_max_error, d_raw_error, d_steps=None, stream=None):
-        """Device pointers (ints); stream is a cudaStream_t as int or None."""
+        """Device pointers (ints); stream is a cudaStream_t as int, or None for
+        the evaluator's own stream (a handle of 0 also maps to it)."""
         _check(self.ev.lib.grn_run_packed(self.ev.ctx, self.handle, ctypes.c_void_p(d_max_error),
                                           ctypes.c_void_p(d_raw_error),
                                           ctypes.c_void_p(d_steps) if d_steps else None,
-                                          ctypes.c_void_p(stream) if stream else None), self.ev.ctx)
+                                          ctypes.c_void_p(stream) if stream is not None else None),
+               self.ev.ctx)
 
     def free(self):
         if self.handle:

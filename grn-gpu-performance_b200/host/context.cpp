@@ -70,6 +70,10 @@ struct grn_ctx {
   std::vector<Job *> free_jobs;
   int forced_schedule = GRN_SCHEDULE_AUTO;
   int forced_threads = 0;
+  // minConc is 0 and the uploaded initial states are finite and
+  // non-negative: the kernel's fast path then gives the same results as the
+  // exact one (see the kernel's update_cell).
+  bool fast_ok = false;
 };
 
 struct grn_packed {
@@ -170,79 +174,54 @@ int host_threads() {
   return n ? (int)n : 1;
 }
 
-// Autotuner, first stage: every compiled kernel variant that can hold the
+// Autotuner, first stage: every compiled kernel variant that can run the
 // batch is scored by its resident useful threads per SM (occupancy x
-// threads that own a group); layouts that double-buffer every gene (one
-// barrier per step) are preferred over ones that hold some genes' new values
-// in registers (two barriers per step).
+// threads that own a group), fixed items preferred over walking ones and
+// all-shared-memory state over state spilling to global slots.
 grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *out) {
   const int W = ctx->p.dim_x, H = ctx->p.dim_y;
   const int Wg = (W + 3) / 4, Q = H * Wg;
-  const size_t plane_bytes = (size_t)H * Wg * 4 * sizeof(float);
+  const bool ragged = (W % 4) != 0;
+  const size_t plane_bytes = (size_t)grn::plane_floats(W, H) * sizeof(float);
   const size_t fixed = grn::sim_fixed_smem_bytes();
   const size_t optin = (size_t)ctx->smem_optin;
-  const int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) : 0;
+  int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) : 0;
+  fit &= ~1;
+  const int sched = ctx->forced_schedule;
   double best_score = -1;
   LaunchPlan best{};
   const int nv = grn::sim_variant_count();
-  if (ctx->forced_schedule != GRN_SCHEDULE_GLOBAL) {
-    for (int i = 0; i < nv; ++i) {
-      grn::KernelVariant v = grn::sim_variant(i);
-      if (v.global_state || v.gmax < max_genes) continue;
-      if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
-      // Candidate plane counts: as many as useful, or the fewest this
-      // variant can run with (more blocks per SM).
-      const int cands[2] = {std::min(fit, 2 * max_genes),
-                            std::max(max_genes, 2 * max_genes - v.nreg)};
-      for (int planes : cands) {
-        if (planes < max_genes || planes > fit) continue;
-        const int n_reg = std::max(0, 2 * max_genes - planes);
-        if (n_reg > v.nreg) continue;
-        if (n_reg > 0 && Q > v.threads * v.items) continue;
-        if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_2BUF && n_reg > 0) continue;
-        if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_1BUF && n_reg == 0) continue;
-        const size_t smem = fixed + planes * plane_bytes;
-        int occ = 0;
-        GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &occ));
-        if (occ < 1) continue;
-        double score = (double)occ * std::min(v.threads, Q) * (n_reg == 0 ? 1.25 : 1.0);
-        score -= 1e-3 * (v.gmax + v.nreg);  // prefer the tighter register footprint
-        if (score > best_score) {
-          best_score = score;
-          best.v = v;
-          best.v.schedule = n_reg == 0 ? GRN_SCHEDULE_SMEM_2BUF : GRN_SCHEDULE_SMEM_1BUF;
-          best.planes = planes;
-          best.smem_bytes = smem;
-          best.blocks_per_sm = occ;
-        }
-      }
-    }
-  }
-  if (best_score < 0) {
-    if (ctx->forced_schedule == GRN_SCHEDULE_SMEM_1BUF ||
-        ctx->forced_schedule == GRN_SCHEDULE_SMEM_2BUF)
-      return fail(ctx, GRN_ERR_CAPACITY, "forced shared-memory schedule cannot hold the grid");
-    // Global-memory state slots.
-    for (int i = 0; i < nv; ++i) {
-      grn::KernelVariant v = grn::sim_variant(i);
-      if (!v.global_state || v.gmax < max_genes) continue;
-      if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
-      int occ = 0;
-      GRN_CUDA(ctx, grn::sim_occupancy(v, fixed, &occ));
-      if (occ < 1) continue;
-      double score = (double)occ * v.threads - 1e-3 * v.gmax;
-      if (score > best_score) {
-        best_score = score;
-        best.v = v;
-        best.planes = 0;
-        best.smem_bytes = fixed;
-        best.blocks_per_sm = occ;
-      }
+  for (int i = 0; i < nv; ++i) {
+    const grn::KernelVariant v = grn::sim_variant(i);
+    if (v.gmax < max_genes || v.ragged != ragged) continue;
+    if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
+    if (!v.loop && Q > v.threads * v.items) continue;
+    if (sched == GRN_SCHEDULE_FIXED_ITEMS && v.loop) continue;
+    if ((sched == GRN_SCHEDULE_WALK_ITEMS || sched == GRN_SCHEDULE_GLOBAL) && !v.loop) continue;
+    const int planes = sched == GRN_SCHEDULE_GLOBAL ? 0 : std::min(fit, 2 * max_genes);
+    const bool spills = planes / 2 < max_genes;
+    const size_t smem = fixed + planes * plane_bytes;
+    int occ = 0;
+    GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &occ));
+    if (occ < 1) continue;
+    double score = (double)occ * std::min(v.threads, Q) * (v.loop ? 1.0 : 1.25) *
+                   (spills ? 0.8 : 1.0);
+    score -= 1e-3 * v.gmax;  // prefer the tighter register footprint
+    if (score > best_score) {
+      best_score = score;
+      best.v = v;
+      best.schedule = sched == GRN_SCHEDULE_GLOBAL ? GRN_SCHEDULE_GLOBAL
+                      : v.loop                     ? GRN_SCHEDULE_WALK_ITEMS
+                                                   : GRN_SCHEDULE_FIXED_ITEMS;
+      best.planes = planes;
+      best.smem_bytes = smem;
+      best.blocks_per_sm = occ;
+      best.slot_floats = spills ? 2LL * v.gmax * grn::plane_floats(W, H) : 0;
     }
   }
   if (best_score < 0)
-    return fail(ctx, GRN_ERR_CAPACITY, "no kernel variant holds " +
-                                           std::to_string(max_genes) + " genes");
+    return fail(ctx, GRN_ERR_CAPACITY, "no kernel variant holds " + std::to_string(max_genes) +
+                                           " genes on this grid with this schedule");
   best.blocks = std::max(1, std::min(n_models, ctx->n_sm * best.blocks_per_sm));
   *out = best;
   return GRN_OK;
@@ -287,12 +266,12 @@ grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_of
   a.error_flag = d_flag;
   a.state_out = d_states;
   a.state_planes = state_planes;
-  if (plan.v.global_state) {
-    const int64_t slot = 2LL * plan.v.gmax * H * Wg * 4;
-    s = ensure_dev(ctx, &ctx->d_gstate, (size_t)slot * plan.blocks * sizeof(float));
+  a.fast_ok = ctx->fast_ok ? 1 : 0;
+  if (plan.slot_floats > 0) {
+    s = ensure_dev(ctx, &ctx->d_gstate, (size_t)plan.slot_floats * plan.blocks * sizeof(float));
     if (s != GRN_OK) return s;
     a.gstate = static_cast<float *>(ctx->d_gstate.p);
-    a.slot_floats = slot;
+    a.slot_floats = plan.slot_floats;
   }
   GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int32_t), stream));
   GRN_CUDA(ctx, grn::sim_launch(plan, a, stream));
@@ -360,7 +339,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
     stats->pack_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     stats->h2d_bytes = (int64_t)(wb + ob + eb);
     stats->d2h_bytes = (int64_t)(eb + sb + 4);
-    stats->schedule = plan.v.schedule;
+    stats->schedule = plan.schedule;
     stats->threads_per_block = plan.v.threads;
     stats->blocks = plan.blocks;
   }
@@ -508,6 +487,12 @@ grn_status grn_set_experiments(grn_ctx *ctx, int n_experiments, const double *in
                                         cudaMemcpyHostToDevice, ctx->stream));
   GRN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->n_exp = n_experiments;
+  bool ok = ctx->p.min_conc == 0.0;
+  for (size_t i = 0; ok && i < ni; ++i) {
+    const double v = fi[i];  // the value the kernel starts from
+    ok = std::isfinite(v) && v >= 0;
+  }
+  ctx->fast_ok = ok;
   return GRN_OK;
 }
 

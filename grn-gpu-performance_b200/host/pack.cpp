@@ -48,7 +48,7 @@ grn_status pack_model(const grn_product *products, int n_products,
   hdr.orig_index = orig_index;
   hdr.n_genes = (int16_t)G;
   hdr.lg_mask = 0;
-  hdr.flags = kFlagNone;
+  hdr.flags = kFlagFast;  // cleared below if a link or rate could make NaN
   std::vector<PackedGene> genes(G);
   std::vector<PackedLink> plinks;
   plinks.reserve(n_links);
@@ -73,6 +73,8 @@ grn_status pack_model(const grn_product *products, int n_products,
     g.deg = (float)prod->deg;
     // The product diffuses iff dif > 0 (cmodelsimulator.cpp:143-147).
     g.dif = prod->dif > 0 ? (float)prod->dif : 0.0f;
+    if (!std::isfinite(g.lim) || !std::isfinite(g.deg) || !std::isfinite(g.dif))
+      hdr.flags &= ~kFlagFast;
     if (g.dif > 0) ++c.dif_genes;
 
     // OR links first, then AND links, each in model link order; a link is
@@ -100,6 +102,9 @@ grn_status pack_model(const grn_product *products, int n_products,
       // activation with n = hillCoef, else repression with n = -hillCoef.
       const bool act = lk->hill_coef >= 0;
       const double n = act ? lk->hill_coef : -1.0 * lk->hill_coef;
+      if (!std::isfinite(n) || !(lk->dis_const > 0) || !std::isfinite(lk->dis_const) ||
+          !std::isfinite((float)(n * std::log2(lk->dis_const))))
+        hdr.flags &= ~kFlagFast;
       if (n == 0) {
         pl.slot = kConstSlot;  // pow(x, 0) = pow(K, 0) = 1: Hill value 1/2
         pl.a = 0.0f;

@@ -150,16 +150,17 @@ typedef struct grn_eval_stats {
   int32_t reserved0;
 } grn_eval_stats;
 
-/* Kernel schedules.  GRN_SCHEDULE_AUTO lets the autotuner pick. */
+/* Kernel schedules.  GRN_SCHEDULE_AUTO lets the autotuner pick.  Every
+ * schedule double-buffers each gene's state plane: in shared memory as far
+ * as it fits, the remaining genes in a per-block global-memory slot. */
 typedef enum grn_schedule {
   GRN_SCHEDULE_AUTO = 0,
-  GRN_SCHEDULE_SMEM_1BUF = 1,  /* one CTA per model, state in shared memory,
-                                  new values held in registers            */
-  GRN_SCHEDULE_SMEM_2BUF = 2,  /* one CTA per model, double-buffered state
-                                  in shared memory                        */
-  GRN_SCHEDULE_GLOBAL = 3      /* one CTA per model, double-buffered state
-                                  in global memory (grids too large for
-                                  shared memory)                          */
+  GRN_SCHEDULE_FIXED_ITEMS = 1, /* each thread owns fixed float4 groups of
+                                   4 cells for the whole launch           */
+  GRN_SCHEDULE_WALK_ITEMS = 2,  /* threads walk the grid's groups; any
+                                   grid size                              */
+  GRN_SCHEDULE_GLOBAL = 3       /* walking groups, every plane in global
+                                   memory                                 */
 } grn_schedule;
 
 typedef struct grn_ctx grn_ctx;
