@@ -303,7 +303,10 @@ def test_run_packed_device_buffers():
         me = torch.full((64,), 1000.0, dtype=torch.float64, device="cuda")
         raw = torch.zeros(64, dtype=torch.float64, device="cuda")
         steps = torch.zeros(64, dtype=torch.int32, device="cuda")
-        s = torch.cuda.current_stream()
+        # A stream of its own: the legacy default stream's handle is 0, which
+        # the C ABI reads as "the evaluator's stream".
+        s = torch.cuda.Stream()
+        torch.cuda.synchronize()
         pk.run(me.data_ptr(), raw.data_ptr(), steps.data_ptr(), s.cuda_stream)
         s.synchronize()
         assert np.array_equal(raw.cpu().numpy(), raw_ref)
