@@ -99,6 +99,9 @@ _SIGNATURES = {
     "grn_packed_get_info": ([_P, ctypes.POINTER(PackedInfo)], _I),
     "grn_run_packed": ([_P, _P, _P, _P, _P, _P], _I),
     "grn_describe_model": ([_P, _I, _P, _I, _I, ctypes.c_char_p, _I], _I),
+    "grn_evaluate_batch_noalloc": ([ctypes.POINTER(SimParams), _I, _P, _P,
+                                    ctypes.POINTER(ModelBatchC), _P, _P, _P, _P,
+                                    ctypes.c_char_p, _I], _I),
 }
 
 _lib = None
@@ -206,6 +209,26 @@ def _check(status, ctx=None):
         if ctx:
             msg = load_library().grn_last_error(ctx).decode()
         raise GrnError(status, msg)
+
+
+def evaluate_batch_noalloc(params, n_experiments, d_initial, d_target, batch, d_max_error,
+                           d_raw_error, d_steps=None, stream=None):
+    """grn_evaluate_batch_noalloc: device pointers (ints) for the experiments,
+    max errors in and raw errors / steps out; `batch` is a host ModelBatch.
+    Allocates no device memory; asynchronous on `stream` (cudaStream_t as int,
+    None = legacy default stream)."""
+    lib = load_library()
+    p = SimParams.from_dict(params)
+    cb = batch.as_c()
+    buf = ctypes.create_string_buffer(512)
+    st = lib.grn_evaluate_batch_noalloc(ctypes.byref(p), int(n_experiments),
+                                        ctypes.c_void_p(d_initial), ctypes.c_void_p(d_target),
+                                        ctypes.byref(cb), ctypes.c_void_p(d_max_error),
+                                        ctypes.c_void_p(d_raw_error),
+                                        ctypes.c_void_p(d_steps) if d_steps else None,
+                                        ctypes.c_void_p(stream) if stream else None, buf, len(buf))
+    if st != GRN_OK:
+        raise GrnError(st, buf.value.decode())
 
 
 class Evaluator:

@@ -306,6 +306,52 @@ grn_status grn_describe_model(const grn_product *products, int n_products,
                               const grn_link *links, int n_links,
                               int n_morphogens, char *buf, int buf_len);
 
+/* ------------------------------------------------ no-allocation entry ---
+ * Device memory that grn_evaluate_batch_noalloc uses instead of allocating:
+ * reserved once on every GPU that loads the library and held until the
+ * process exits. */
+#define GRN_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Batch evaluation that allocates no device memory.  No counterpart in the
+ * reference (its evaluator allocates per thread and per model size).
+ *
+ * For callers that cannot allocate GPU memory: a host application that has
+ * already divided the device memory among its components and passes this
+ * library only buffers it owns, or a long-running search loop that must not
+ * block in, or fail out of, the device allocator in the middle of a run.
+ *
+ * Runs the same simulation kernel as grn_evaluate_batch on the calling
+ * thread's current device, asynchronously on `cuda_stream` (NULL = the
+ * legacy default stream).  The caller passes every input and output:
+ *   d_initial  [n_experiments][n_input_morphogens][dim_y][dim_x]  FP32, device
+ *   d_target   [n_experiments][n_target_morphogens][dim_y][dim_x] FP32, device
+ *   batch      models in genome form, host memory (compiled on the host)
+ *   d_max_error [n_models] device in; d_raw_error [n_models] device out
+ *   (unrounded, round with grn_round_error); d_steps [n_models] device out
+ *   or NULL.
+ * Everything else -- work counter, error flag, compiled records, state slots
+ * of genes that do not fit in shared memory -- lives in a fixed device array
+ * of GRN_NOALLOC_SCRATCH_BYTES.  A batch whose records do not fit in it, or
+ * a grid one block's state slot does not fit in, is rejected with
+ * GRN_ERR_CAPACITY and a message in err_buf; when the slots of one block per
+ * SM do not fit, fewer persistent blocks run.  No cudaMalloc, cudaFree or
+ * other allocating device routine is called.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the array and it keeps the previous call's contents;
+ * the call clears what must start at zero.  Calls whose GPU work overlaps
+ * (other streams, or other threads) race on the array: serialise them.
+ * A model record the kernel rejects yields a NaN raw error.  Uses the
+ * kernel's exact arithmetic path only.  err_buf (may be NULL) receives a
+ * one-line description of a failure. */
+grn_status grn_evaluate_batch_noalloc(const grn_sim_params *params, int n_experiments,
+                                      const float *d_initial, const float *d_target,
+                                      const grn_model_batch *batch,
+                                      const double *d_max_error, double *d_raw_error,
+                                      int32_t *d_steps, void *cuda_stream,
+                                      char *err_buf, int err_buf_len);
+
 /* Rounds a raw error the way the reference's evaluate does:
  * 100 if raw > max_error, else ceilS(raw, precision)
  * (Src/Common/mathalgo.h:55-62). */
