@@ -66,8 +66,26 @@ struct ModelSmem {
 constexpr int kModelWords = sizeof(ModelSmem) / 16;
 static_assert(sizeof(ModelSmem) % 16 == 0, "model smem is whole words");
 
+// Dense form of a fast model's regulation, built in shared memory when the
+// model is loaded: for gene p, the regulator slots of its OR links and of
+// its AND links as bitmasks, and the (a, b) of the link from slot k at
+// ab[p][k].  Hill-coefficient-0 links (constant term 0) fold into or_init
+// (min with 0) and and_floor (max with 0).
+struct DenseGene {
+  uint32_t or_slots;
+  uint32_t and_slots;
+  float or_init;    // +inf, or 0 with a constant OR term
+  float and_floor;  // -inf, or 0 with a constant AND term
+};
+struct DenseSmem {
+  DenseGene gene[GRN_MAX_GENES];
+  float2 ab[GRN_MAX_GENES][GRN_MAX_GENES];
+};
+static_assert(sizeof(DenseSmem) % 16 == 0, "dense table is whole words");
+
 // Fixed shared-memory layout in front of the state planes.
-constexpr size_t kRedOffset = sizeof(ModelSmem);         // float [2][32]
+constexpr size_t kDenseOffset = sizeof(ModelSmem);
+constexpr size_t kRedOffset = kDenseOffset + sizeof(DenseSmem);  // float [2][32]
 constexpr size_t kDredOffset = kRedOffset + 2 * 32 * 4;  // double [32]
 constexpr size_t kWorkOffset = kDredOffset + 32 * 8;     // int
 constexpr size_t kStateOffset = (kWorkOffset + 16 + 127) & ~size_t(127);
@@ -169,6 +187,91 @@ __device__ __forceinline__ void regulation(const ModelSmem &M, const PackedGene 
   }
 }
 
+// Regulation of gene p for NI groups from the dense table (fast models):
+// regulator slots are a compile-time loop, so the lg2 values are read with
+// fixed register indices and no per-link dispatch is needed.  The result is
+// the fast combine's: min over OR terms, then max with each AND term (terms
+// are never NaN for fast models, and min/max are order-free).
+template <int NI, int GMAX>
+__device__ __forceinline__ void regulation_dense(const ModelSmem &M, const DenseSmem &D, int p,
+                                                 const float4 (&lg)[NI][GMAX],
+                                                 float4 (&h)[NI]) {
+  const PackedGene &g = M.genes[p];
+  if (g.n_or + g.n_and == 0) {  // OpZero
+#pragma unroll
+    for (int i = 0; i < NI; ++i) h[i] = f4(0.0f);
+    return;
+  }
+  const DenseGene dg = D.gene[p];
+  float4 v[NI];
+#pragma unroll
+  for (int i = 0; i < NI; ++i) v[i] = f4(dg.or_init);
+  const uint32_t os = dg.or_slots, as = dg.and_slots;
+#pragma unroll
+  for (int k = 0; k < GMAX; ++k) {
+    if ((os >> k) == 0u) break;
+    if ((os >> k) & 1u) {
+      const float2 ab = D.ab[p][k];
+#pragma unroll
+      for (int i = 0; i < NI; ++i) comb4<kOrFast>(v[i], ab.x, lg[i][k], ab.y);
+    }
+  }
+  if (g.n_or == 0) {
+#pragma unroll
+    for (int i = 0; i < NI; ++i) v[i] = f4(dg.and_floor);
+  } else {
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      v[i].x = fmaxf(v[i].x, dg.and_floor);
+      v[i].y = fmaxf(v[i].y, dg.and_floor);
+      v[i].z = fmaxf(v[i].z, dg.and_floor);
+      v[i].w = fmaxf(v[i].w, dg.and_floor);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < GMAX; ++k) {
+    if ((as >> k) == 0u) break;
+    if ((as >> k) & 1u) {
+      const float2 ab = D.ab[p][k];
+#pragma unroll
+      for (int i = 0; i < NI; ++i) comb4<kAndFast>(v[i], ab.x, lg[i][k], ab.y);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    h[i].x = rcp_approx(1.0f + ex2_approx(v[i].x));
+    h[i].y = rcp_approx(1.0f + ex2_approx(v[i].y));
+    h[i].z = rcp_approx(1.0f + ex2_approx(v[i].z));
+    h[i].w = rcp_approx(1.0f + ex2_approx(v[i].w));
+  }
+}
+
+// Builds the dense table of a fast model (one thread per gene).
+__device__ __forceinline__ void build_dense(const ModelSmem &M, DenseSmem &D, int tid) {
+  const int G = M.hdr.n_genes;
+  if (tid < G) {
+    const PackedGene g = M.genes[tid];
+    DenseGene dg;
+    dg.or_slots = 0u;
+    dg.and_slots = 0u;
+    dg.or_init = __int_as_float(0x7f800000);
+    dg.and_floor = __int_as_float(0xff800000);
+    for (int l = 0; l < g.n_or + g.n_and; ++l) {
+      const PackedLink lk = M.links[g.link_begin + l];
+      const bool is_or = l < g.n_or;
+      if (lk.slot == kConstSlot) {
+        if (is_or) dg.or_init = fminf(dg.or_init, 0.0f);
+        else dg.and_floor = fmaxf(dg.and_floor, 0.0f);
+      } else {
+        if (is_or) dg.or_slots |= 1u << lk.slot;
+        else dg.and_slots |= 1u << lk.slot;
+        D.ab[tid][lk.slot] = make_float2(lk.a, lk.b);
+      }
+    }
+    D.gene[tid] = dg;
+  }
+}
+
 // ---- geometry ----------------------------------------------------------
 //
 // A state plane holds the W x H grid as rows of RS = 4 * Wg floats (rows
@@ -259,12 +362,16 @@ __device__ __forceinline__ float update_cell(float c, float h, float lim, float 
 // plane (shared or global memory).  All lanes of a warp call this together
 // (it shuffles).  `mx` takes the max |rate| of the valid groups' real cells.
 template <int NI, int GMAX, bool EXACT, bool RAGGED>
-__device__ __forceinline__ void gene_update(const ModelSmem &M, const PackedGene &gn,
+__device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem &D, int p,
+                                            const PackedGene &gn,
                                             const float4 (&lg)[NI][GMAX], const float *cur,
                                             const Geom &g, const Item (&it)[NI], float dt,
                                             float min_conc, float &mx, float4 (&nv)[NI]) {
   float4 h[NI];
-  regulation<NI, GMAX, EXACT>(M, gn, lg, h);
+  if constexpr (EXACT)
+    regulation<NI, GMAX, true>(M, gn, lg, h);
+  else
+    regulation_dense<NI, GMAX>(M, D, p, lg, h);
   const bool diffuses = gn.dif > 0.0f;  // uniform: the same gene for the whole block
 #pragma unroll
   for (int i = 0; i < NI; ++i) {
@@ -356,7 +463,8 @@ __device__ __forceinline__ float *plane_of(const StatePtrs &sp, const Geom &g, i
 // New values of all genes of NI groups: shared-memory genes first, then
 // global-memory genes (two loops so that each uses its own load path).
 template <int NI, int GMAX, bool EXACT, bool RAGGED>
-__device__ __forceinline__ void group_step(const ModelSmem &M, const StatePtrs &sp,
+__device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &D,
+                                           const StatePtrs &sp,
                                            const Geom &g, const Item (&it)[NI], int par,
                                            float dt, float min_conc, float &mx) {
   const int G = M.hdr.n_genes;
@@ -365,12 +473,16 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const StatePtrs &
   float *sm_nxt = sp.sm + (par ? 0 : sp.n_sm) * g.PS;
   const float *gl_cur = sp.gl + (par ? GMAX : 0) * g.PS;
   float *gl_nxt = sp.gl + (par ? 0 : GMAX) * g.PS;
-  // lg2 of every regulator gene's current value (0 for genes no link reads).
+  // lg2 of every regulator gene's current value.  The dense (fast) path
+  // reads an entry only under its slot bit, so entries of genes no link
+  // reads are left unset there; the exact path's slot switch needs them 0.
   float4 lg[NI][GMAX];
 #pragma unroll
   for (int k = 0; k < GMAX; ++k) {
+    {
 #pragma unroll
-    for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
+      for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
+    }
     if (k < G && ((lg_mask >> k) & 1u)) {
       const float *pl = (k < sp.n_sm ? sm_cur : gl_cur) + k * g.PS;
 #pragma unroll
@@ -386,8 +498,8 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const StatePtrs &
   for (int p = 0; p < sp.n_sm; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GMAX, EXACT, RAGGED>(M, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc, mx,
-                                         nv);
+    gene_update<NI, GMAX, EXACT, RAGGED>(M, D, p, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc,
+                                         mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(sm_nxt + p * g.PS + it[i].base) = nv[i];
@@ -395,8 +507,8 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const StatePtrs &
   for (int p = sp.n_sm; p < G; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GMAX, EXACT, RAGGED>(M, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc, mx,
-                                         nv);
+    gene_update<NI, GMAX, EXACT, RAGGED>(M, D, p, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc,
+                                         mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(gl_nxt + p * g.PS + it[i].base) = nv[i];
@@ -415,6 +527,7 @@ template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
+  DenseSmem &D = *reinterpret_cast<DenseSmem *>(smem + kDenseOffset);
   float *s_red = reinterpret_cast<float *>(smem + kRedOffset);
   double *s_dred = reinterpret_cast<double *>(smem + kDredOffset);
   int *s_work = reinterpret_cast<int *>(smem + kWorkOffset);
@@ -480,6 +593,11 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       continue;
     }
 
+    if (!exact) {
+      build_dense(M, D, tid);
+      __syncthreads();
+    }
+
     double error = 0.0, change_sum = 0.0;
     int steps_total = 0;
     const double max_err = A.max_error[orig];
@@ -510,9 +628,9 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
           // All ITEMS groups of the thread at once (items past the grid are
           // clamped duplicates and store nothing).
           if (exact)
-            group_step<ITEMS, GMAX, true, RAGGED>(M, sp, g, items, par, dt, min_conc, mx);
+            group_step<ITEMS, GMAX, true, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
           else
-            group_step<ITEMS, GMAX, false, RAGGED>(M, sp, g, items, par, dt, min_conc, mx);
+            group_step<ITEMS, GMAX, false, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
         } else {
           int y = y0, gx = gx0;
           for (int i = 0; i < n_iter; ++i) {
@@ -520,9 +638,9 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
             const bool valid = q < g.Q;
             const Item it[1] = {valid ? make_item(y, gx, true, lane, g) : item_at(q, lane, g)};
             if (exact)
-              group_step<1, GMAX, true, RAGGED>(M, sp, g, it, par, dt, min_conc, mx);
+              group_step<1, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
             else
-              group_step<1, GMAX, false, RAGGED>(M, sp, g, it, par, dt, min_conc, mx);
+              group_step<1, GMAX, false, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
             y += dy;
             gx += dgx;
             if (gx >= g.Wg) {

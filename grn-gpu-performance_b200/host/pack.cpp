@@ -129,6 +129,23 @@ grn_status pack_model(const grn_product *products, int n_products,
     }
     if (g.n_or + g.n_and > 0) ++c.reg_genes;
   }
+  // The kernel's dense regulation holds one link per (regulated, regulator)
+  // pair; a model with a repeated pair takes the exact path.
+  for (size_t i = 0; i < plinks.size() && (hdr.flags & kFlagFast); ++i)
+    for (size_t j = i + 1; j < plinks.size(); ++j)
+      if (plinks[i].slot == plinks[j].slot && plinks[i].slot != kConstSlot) {
+        // same slot twice within one gene's link range?
+        int gi = -1, gj = -1;
+        for (int q = 0; q < G; ++q) {
+          const int b = genes[q].link_begin, e = b + genes[q].n_or + genes[q].n_and;
+          if ((int)i >= b && (int)i < e) gi = q;
+          if ((int)j >= b && (int)j < e) gj = q;
+        }
+        if (gi == gj) {
+          hdr.flags &= ~kFlagFast;
+          break;
+        }
+      }
   hdr.n_links = (int16_t)plinks.size();
   c.links = (int)plinks.size();
   c.lg_genes = __builtin_popcount(hdr.lg_mask);
