@@ -49,6 +49,24 @@ class SimParams(ctypes.Structure):
         return p
 
 
+class EvolutionParams(ctypes.Structure):
+    _fields_ = [("n_demes", ctypes.c_int32), ("deme_size", ctypes.c_int32),
+                ("migration_period", ctypes.c_int32), ("n_max_products", ctypes.c_int32),
+                ("n_max_links", ctypes.c_int32), ("n_host_threads", ctypes.c_int32),
+                ("seed", ctypes.c_uint64)]
+
+
+class GenerationStats(ctypes.Structure):
+    _fields_ = [("generation", ctypes.c_int32), ("n_evaluated", ctypes.c_int32),
+                ("best_error", ctypes.c_double), ("best_complexity", ctypes.c_int32),
+                ("pareto_size", ctypes.c_int32), ("mean_error", ctypes.c_double),
+                ("host_ms", ctypes.c_double), ("eval_ms", ctypes.c_double),
+                ("migrated", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
+
+
 class ModelBatchC(ctypes.Structure):
     _fields_ = [("n_models", ctypes.c_int32), ("reserved0", ctypes.c_int32),
                 ("product_offsets", ctypes.c_void_p), ("products", ctypes.c_void_p),
@@ -77,6 +95,9 @@ class PackedInfo(ctypes.Structure):
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
+# grn_error_calculator_fn
+CALCULATOR_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ModelBatchC),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double))
 _SIGNATURES = {
     "grn_abi_version": ([], _I),
     "grn_status_str": ([_I], ctypes.c_char_p),
@@ -99,6 +120,14 @@ _SIGNATURES = {
     "grn_packed_get_info": ([_P, ctypes.POINTER(PackedInfo)], _I),
     "grn_run_packed": ([_P, _P, _P, _P, _P, _P], _I),
     "grn_describe_model": ([_P, _I, _P, _I, _I, ctypes.c_char_p, _I], _I),
+    "grn_evolution_create": ([ctypes.POINTER(EvolutionParams), _I, _P, ctypes.POINTER(_P)], _I),
+    "grn_evolution_create_cb": ([ctypes.POINTER(EvolutionParams), _I, CALCULATOR_FN, _P,
+                                 ctypes.POINTER(_P)], _I),
+    "grn_evolution_step": ([_P, ctypes.POINTER(GenerationStats)], _I),
+    "grn_evolution_individual": ([_P, _I, _I, _P, _I, ctypes.POINTER(_I), _P, _I,
+                                  ctypes.POINTER(_I), ctypes.POINTER(_D), ctypes.POINTER(_I)], _I),
+    "grn_evolution_best": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "grn_evolution_destroy": ([_P], _I),
     "grn_evaluate_batch_noalloc": ([ctypes.POINTER(SimParams), _I, _P, _P,
                                     ctypes.POINTER(ModelBatchC), _P, _P, _P, _P,
                                     ctypes.c_char_p, _I], _I),
@@ -363,5 +392,85 @@ class Packed:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+def batch_from_c(cb):
+    """ModelBatch copy of a grn_model_batch passed to a calculator callback."""
+    n = cb.contents.n_models
+    po = np.ctypeslib.as_array(ctypes.cast(cb.contents.product_offsets,
+                                           ctypes.POINTER(ctypes.c_int32)), (n + 1,)).copy()
+    lo = np.ctypeslib.as_array(ctypes.cast(cb.contents.link_offsets,
+                                           ctypes.POINTER(ctypes.c_int32)), (n + 1,)).copy()
+    npr, nli = int(po[-1]), int(lo[-1])
+    prods = np.frombuffer(ctypes.string_at(cb.contents.products, npr * PRODUCT_DTYPE.itemsize),
+                          PRODUCT_DTYPE).copy() if npr else np.zeros(0, PRODUCT_DTYPE)
+    links = np.frombuffer(ctypes.string_at(cb.contents.links, nli * LINK_DTYPE.itemsize),
+                          LINK_DTYPE).copy() if nli else np.zeros(0, LINK_DTYPE)
+    return ModelBatch(po, prods, lo, links)
+
+
+class Evolution:
+    """Island search (grn_evolution_*).  Pass an Evaluator to evaluate on the
+    GPU, or a Python callable calculator(batch, max_error) -> errors."""
+
+    def __init__(self, params, n_morphogens, evaluator=None, calculator=None):
+        self.lib = load_library()
+        self._p = EvolutionParams(**params)
+        h = ctypes.c_void_p()
+        if evaluator is not None:
+            self._keep = evaluator
+            _check(self.lib.grn_evolution_create(ctypes.byref(self._p), n_morphogens,
+                                                 evaluator.ctx, ctypes.byref(h)))
+        else:
+            def trampoline(user, cb, max_error, error_out):
+                try:
+                    batch = batch_from_c(cb)
+                    n = batch.n_models
+                    me = np.ctypeslib.as_array(max_error, (n,)).copy()
+                    out = np.asarray(calculator(batch, me), np.float64)
+                    np.ctypeslib.as_array(error_out, (n,))[:] = out
+                    return GRN_OK
+                except Exception:  # surfaced as a status, not an unwind through C
+                    import traceback
+                    traceback.print_exc()
+                    return 3
+            self._cb = CALCULATOR_FN(trampoline)
+            _check(self.lib.grn_evolution_create_cb(ctypes.byref(self._p), n_morphogens,
+                                                    self._cb, None, ctypes.byref(h)))
+        self.handle = h
+
+    def step(self):
+        st = GenerationStats()
+        _check(self.lib.grn_evolution_step(self.handle, ctypes.byref(st)))
+        return st.as_dict()
+
+    def individual(self, deme, index):
+        npr, nli, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        err = ctypes.c_double()
+        _check(self.lib.grn_evolution_individual(self.handle, deme, index, None, 0,
+                                                 ctypes.byref(npr), None, 0, ctypes.byref(nli),
+                                                 ctypes.byref(err), ctypes.byref(c)))
+        prods = np.zeros(npr.value, PRODUCT_DTYPE)
+        links = np.zeros(nli.value, LINK_DTYPE)
+        _check(self.lib.grn_evolution_individual(self.handle, deme, index, _ptr(prods),
+                                                 npr.value, None, _ptr(links), nli.value, None,
+                                                 None, None))
+        return prods, links, err.value, c.value
+
+    def best(self):
+        d, i = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.grn_evolution_best(self.handle, ctypes.byref(d), ctypes.byref(i)))
+        return d.value, i.value
+
+    def close(self):
+        if self.handle:
+            self.lib.grn_evolution_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

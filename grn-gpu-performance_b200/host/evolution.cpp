@@ -1,0 +1,630 @@
+// evolution.cpp -- island evolutionary search on top of a batched evaluator.
+//
+// Model operators restate Src/Model/model.cpp (cross :21-85, copyLinks
+// :120-184, createRandom :285-315, duplicateProduct :317-333, mutate
+// :499-547, removeExcess :550-574), Src/Model/modelprod.cpp:14-59 and
+// Src/Model/modellink.cpp:10-53.  Where the reference iterates a QSet (hash
+// order) this code iterates labels in ascending order.  The search restates
+// SearchAlgoDetCrowd (Src/Search/searchalgodetcrowd.cpp:54-147) and the
+// migration of Search (Src/Search/search.cpp:263-311), synchronously: every
+// generation all demes reproduce, all children are evaluated in one batch
+// (the GPU evaluator runs them in one persistent launch), then each deme
+// selects and, every migration_period generations, random deme pairs mix.
+
+#include "evolution.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <thread>
+
+namespace grn {
+
+namespace {
+
+bool has(const std::vector<int> &v, int x) { return std::find(v.begin(), v.end(), x) != v.end(); }
+
+std::vector<int> product_labels(const GModel &m) {
+  std::vector<int> l;
+  for (const auto &p : m.prods)
+    if (!has(l, p.label)) l.push_back(p.label);
+  std::sort(l.begin(), l.end());
+  return l;
+}
+
+// ModelProd(nMorphogens, label) (modelprod.cpp:14-24, zeroInit :61-70).
+grn_product random_product(Rng &rng, int label, int n_morph) {
+  grn_product p{};
+  p.label = label;
+  p.init = (label == 0 && n_morph > 0) ? -1 : (label == 1 && n_morph > 1) ? -2
+         : (label == 2 && n_morph > 2) ? -3 : 0;
+  p.lim = rng.rand01();
+  p.deg = rng.rand01();
+  if (rng.rand100() < 10) p.dif = rng.rand01();
+  else p.dif = 0;
+  return p;
+}
+
+// ModelLink(regulator, regulated) with isActivation = false
+// (modellink.cpp:10-22).
+grn_link random_link(Rng &rng, int regulator, int regulated) {
+  grn_link l{};
+  l.regulator = regulator;
+  l.regulated = regulated;
+  l.dis_const = rng.rand01();
+  if (rng.rand_bool()) l.hill_coef = rng.rand15();
+  else l.hill_coef = -1.0 * rng.rand15();
+  l.is_and = (l.hill_coef < 0) || rng.rand_bool();
+  return l;
+}
+
+// Model::removeLink(regulator, regulated): the first matching link.
+void remove_link(GModel *m, int regulator, int regulated) {
+  for (size_t i = 0; i < m->links.size(); ++i)
+    if (m->links[i].regulator == regulator && m->links[i].regulated == regulated) {
+      m->links.erase(m->links.begin() + i);
+      return;
+    }
+}
+
+void add_or_replace_random_link(Rng &rng, GModel *m, int regulator, int regulated) {
+  remove_link(m, regulator, regulated);
+  m->links.push_back(random_link(rng, regulator, regulated));
+}
+
+bool find_link(const GModel &m, int regulator, int regulated) {
+  for (const auto &l : m.links)
+    if (l.regulator == regulator && l.regulated == regulated) return true;
+  return false;
+}
+
+void remove_links_of(GModel *m, int label) {
+  m->links.erase(std::remove_if(m->links.begin(), m->links.end(),
+                                [&](const grn_link &l) {
+                                  return l.regulator == label || l.regulated == label;
+                                }),
+                 m->links.end());
+}
+
+// Model::removeProductWithLabel (model.cpp:352-371).
+void remove_product_with_label(GModel *m, int label) {
+  for (size_t i = 0; i < m->prods.size(); ++i)
+    if (m->prods[i].label == label) {
+      m->prods.erase(m->prods.begin() + i);
+      remove_links_of(m, label);
+      return;
+    }
+}
+
+// Model::distributeProducts (model.cpp:87-99): each label goes to the
+// second set with probability 1/2.
+void distribute(Rng &rng, const std::vector<int> &from, std::vector<int> *to1,
+                std::vector<int> *to2) {
+  for (int l : from) {
+    if (rng.rand100() < 50) to2->push_back(l);
+    else to1->push_back(l);
+  }
+}
+
+std::vector<int> set_union(const std::vector<int> &a, const std::vector<int> &b) {
+  std::vector<int> u = a;
+  for (int x : b)
+    if (!has(u, x)) u.push_back(x);
+  std::sort(u.begin(), u.end());
+  return u;
+}
+
+// Model::copyProductsAndLinks (model.cpp:101-184).
+void copy_products_and_links(Rng &rng, GModel *to, const GModel &from1,
+                             const std::vector<int> &products1, const GModel &from2,
+                             const std::vector<int> &products2, int n_morph) {
+  for (const auto &p : from1.prods)
+    if (has(products1, p.label)) to->prods.push_back(p);
+  for (const auto &p : from2.prods)
+    if (has(products2, p.label)) to->prods.push_back(p);
+  auto regulators = [&](const std::vector<int> &ps) {
+    std::vector<int> r = ps;
+    std::sort(r.begin(), r.end());
+    r.erase(std::remove_if(r.begin(), r.end(), [&](int l) { return l < n_morph; }), r.end());
+    return r;
+  };
+  const std::vector<int> reg1 = regulators(products1), reg2 = regulators(products2);
+  for (const auto &l : from1.links) {
+    if (!has(products1, l.regulated)) continue;
+    if (has(products1, l.regulator) || has(products2, l.regulator)) {
+      to->links.push_back(l);
+    } else if (!reg2.empty()) {
+      const int nr = reg2[rng.rand_int((int)reg2.size())];
+      if (!find_link(from1, nr, l.regulated)) {
+        grn_link c = l;
+        c.regulator = nr;
+        to->links.push_back(c);
+      }
+    }
+  }
+  for (const auto &l : from2.links) {
+    if (!has(products2, l.regulated)) continue;
+    if (has(products2, l.regulator) || has(products1, l.regulator)) {
+      to->links.push_back(l);
+    } else if (!reg1.empty()) {
+      const int nr = reg1[rng.rand_int((int)reg1.size())];
+      if (!find_link(from2, nr, l.regulated)) {
+        grn_link c = l;
+        c.regulator = nr;
+        to->links.push_back(c);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+std::vector<int> labels_in_use(const GModel &m, int n_morph) {
+  std::vector<int> in_use;
+  for (int i = 0; i < n_morph; ++i) in_use.push_back(i);
+  for (size_t h = 0; h < in_use.size(); ++h)
+    for (const auto &l : m.links)
+      if (l.regulated == in_use[h] && !has(in_use, l.regulator)) in_use.push_back(l.regulator);
+  std::sort(in_use.begin(), in_use.end());
+  return in_use;
+}
+
+GModel ModelOps::create_random(Rng &rng, int n_products) const {
+  // Model::createRandom (model.cpp:285-315).
+  GModel m;
+  for (int i = 0; i < n_products; ++i) m.prods.push_back(random_product(rng, i, n_morph));
+  for (int i = 0; i < n_products; ++i) {
+    const int n_reg = rng.rand_int(1 + n_products);
+    for (int j = 0; j < n_reg; ++j) add_or_replace_random_link(rng, &m, i, rng.rand_int(n_products));
+  }
+  return m;
+}
+
+void ModelOps::cross(Rng &rng, const GModel &p1, const GModel &p2, GModel *c1,
+                     GModel *c2) const {
+  // Model::cross (model.cpp:21-85).
+  const std::vector<int> l1 = product_labels(p1), l2 = product_labels(p2);
+  std::vector<int> common, only1, only2;
+  for (int l : l1) (has(l2, l) ? common : only1).push_back(l);
+  for (int l : l2)
+    if (!has(l1, l)) only2.push_back(l);
+  std::vector<int> copied, swapped, e11, e12, e22, e21;
+  distribute(rng, common, &copied, &swapped);
+  distribute(rng, only1, &e11, &e12);
+  distribute(rng, only2, &e22, &e21);
+  GModel a, b;
+  copy_products_and_links(rng, &a, p1, set_union(copied, e11), p2, set_union(swapped, e21), n_morph);
+  copy_products_and_links(rng, &b, p2, set_union(copied, e22), p1, set_union(swapped, e12), n_morph);
+  if (copied.size() + e11.size() < swapped.size() + e21.size()) std::swap(a, b);
+  remove_excess(rng, &a);
+  remove_excess(rng, &b);
+  *c1 = std::move(a);
+  *c2 = std::move(b);
+}
+
+void ModelOps::remove_excess(Rng &rng, GModel *m) const {
+  // Model::removeExcess (model.cpp:550-574), nMinProducts = nMorphogens.
+  if (n_max_prods > -1) {
+    std::vector<int> in_use = labels_in_use(*m, n_morph);
+    const int n_remove = (int)in_use.size() - n_max_prods;
+    if (n_remove > 0) {
+      in_use.erase(std::remove_if(in_use.begin(), in_use.end(),
+                                  [&](int l) { return l >= 0 && l < n_morph; }),
+                   in_use.end());
+      for (int i = 0; i < n_remove && !in_use.empty(); ++i) {
+        const int k = rng.rand_int((int)in_use.size());
+        remove_product_with_label(m, in_use[k]);
+        in_use.erase(in_use.begin() + k);
+      }
+    }
+  }
+  if (n_max_links > -1) {
+    const std::vector<int> in_use = labels_in_use(*m, n_morph);
+    std::vector<int> used;  // indices of links in use, model order
+    for (size_t i = 0; i < m->links.size(); ++i)
+      if (has(in_use, m->links[i].regulator) && has(in_use, m->links[i].regulated))
+        used.push_back((int)i);
+    const int n_remove = (int)used.size() - n_max_links;
+    std::vector<char> drop(m->links.size(), 0);
+    for (int i = 0; i < n_remove; ++i) {
+      const int k = rng.rand_int((int)used.size());
+      drop[used[k]] = 1;
+      used.erase(used.begin() + k);
+    }
+    size_t w = 0;
+    for (size_t i = 0; i < m->links.size(); ++i)
+      if (!drop[i]) m->links[w++] = m->links[i];
+    m->links.resize(w);
+  }
+}
+
+void ModelOps::mutate(Rng &rng, LabelSource &labels, GModel *m) const {
+  // Model::mutate (model.cpp:499-547); nMinProducts = nMorphogens.
+  for (int i = (int)m->prods.size() - 1; i >= 0; --i) {
+    const int label = m->prods[i].label;
+    if (rng.rand100() < 1) {
+      // duplicateProduct (model.cpp:317-333)
+      grn_product np = m->prods[i];
+      np.init = 0;
+      np.label = labels.take();
+      m->prods.push_back(np);
+      add_or_replace_random_link(rng, m, np.label,
+                                 m->prods[rng.rand_int((int)m->prods.size())].label);
+      const std::vector<int> ls = product_labels(*m);
+      const int n_choice = (int)m->prods.size() - n_morph;
+      if (n_choice > 0)
+        add_or_replace_random_link(rng, m, ls[n_morph + rng.rand_int(n_choice)], np.label);
+    }
+    if (label >= n_morph && rng.rand1000() < 15) {
+      // removeProduct(i) (model.cpp:336-350)
+      m->prods.erase(m->prods.begin() + i);
+      remove_links_of(m, label);
+    }
+  }
+  for (int i = (int)m->links.size() - 1; i >= 0; --i) {
+    if (rng.rand100() < 1) {
+      // duplicateLink (model.cpp:472-483)
+      grn_link nl = m->links[i];
+      const int n = (int)m->prods.size();
+      const int regulator = m->prods[rng.rand_int(n)].label;
+      const int regulated = m->prods[rng.rand_int(n)].label;
+      remove_link(m, regulator, regulated);
+      nl.regulator = regulator;
+      nl.regulated = regulated;
+      m->links.push_back(nl);
+    }
+    if (rng.rand1000() < 15 && i < (int)m->links.size()) m->links.erase(m->links.begin() + i);
+  }
+  remove_excess(rng, m);
+  // Parameter mutations with probability 1% each (modelprod.cpp:43-59,
+  // modellink.cpp:30-41).
+  for (auto &p : m->prods) {
+    if (rng.rand100() < 1) p.lim = rng.rand01();
+    if (rng.rand100() < 1) p.deg = rng.rand01();
+    if (rng.rand100() < 1) {
+      if (rng.rand_bool()) p.dif = rng.rand01();
+      else p.dif = 0;
+    }
+  }
+  for (auto &l : m->links) {
+    if (rng.rand100() < 1) l.dis_const = rng.rand01();
+    if (rng.rand100() < 1) {
+      if (rng.rand_bool()) l.hill_coef = rng.rand15();
+      else l.hill_coef = -1.0 * rng.rand15();
+    }
+    if (l.hill_coef < 0) l.is_and = 1;
+    else if (rng.rand100() < 1) l.is_and = rng.rand_bool();
+  }
+}
+
+int ModelOps::complexity_in_use(const GModel &m) const {
+  // Model::calcComplexityInUse (model.cpp:590-611).
+  const std::vector<int> in_use = labels_in_use(m, n_morph);
+  int c = 0;
+  for (const auto &p : m.prods)
+    if (has(in_use, p.label)) c += 1 + (p.dif > 0);
+  for (const auto &l : m.links)
+    if (has(in_use, l.regulator) && has(in_use, l.regulated)) c += 1;
+  return c;
+}
+
+}  // namespace grn
+
+// ------------------------------------------------------------- the search
+
+namespace {
+
+using grn::GModel;
+
+struct Individual {
+  GModel model;
+  double error = -1;
+  double parent_error = 1000;  // Individual.cpp:19-25: random individuals
+  int complexity = 0;
+};
+
+struct Deme {
+  std::vector<Individual> pop;
+  std::vector<Individual> children;
+  std::vector<int> perm;  // randPopulationInd_, shuffled in place every generation
+  grn::Rng rng{0};
+  grn::LabelSource labels{11, 1};
+};
+
+}  // namespace
+
+struct grn_evolution {
+  grn_evolution_params p{};
+  grn::ModelOps ops{};
+  grn_error_calculator_fn fn = nullptr;
+  void *user = nullptr;
+  std::vector<Deme> demes;
+  grn::Rng search_rng{0};
+  int generation = -1;
+  std::string last_error;
+};
+
+namespace {
+
+grn_status evaluate_all(grn_evolution *evo, std::vector<Individual *> &inds) {
+  std::vector<int32_t> po(1, 0), lo(1, 0);
+  std::vector<grn_product> prods;
+  std::vector<grn_link> links;
+  std::vector<double> max_err, err(inds.size());
+  for (Individual *ind : inds) {
+    prods.insert(prods.end(), ind->model.prods.begin(), ind->model.prods.end());
+    links.insert(links.end(), ind->model.links.begin(), ind->model.links.end());
+    po.push_back((int32_t)prods.size());
+    lo.push_back((int32_t)links.size());
+    max_err.push_back(ind->parent_error);
+  }
+  grn_model_batch b{};
+  b.n_models = (int32_t)inds.size();
+  b.product_offsets = po.data();
+  b.products = prods.empty() ? nullptr : prods.data();
+  b.link_offsets = lo.data();
+  b.links = links.empty() ? nullptr : links.data();
+  const grn_status s = evo->fn(evo->user, &b, max_err.data(), err.data());
+  if (s != GRN_OK) return s;
+  for (size_t i = 0; i < inds.size(); ++i) inds[i]->error = err[i];
+  return GRN_OK;
+}
+
+void fill_stats(grn_evolution *evo, grn_generation_stats *st) {
+  double best = 1e300, sum = 0;
+  int best_c = 1 << 30;
+  long n = 0;
+  std::vector<std::pair<double, int>> pts;
+  for (const Deme &d : evo->demes)
+    for (const Individual &ind : d.pop) {
+      sum += ind.error;
+      ++n;
+      if (ind.error < best || (ind.error == best && ind.complexity < best_c)) {
+        best = ind.error;
+        best_c = ind.complexity;
+      }
+      pts.push_back({ind.error, ind.complexity});
+    }
+  // Non-dominated (error, complexity) points, duplicates included
+  // (Search::recalculateParetoFront, search.cpp:349-377).
+  std::sort(pts.begin(), pts.end());
+  int pareto = 0;
+  double last_e = 0;
+  int last_c = 1 << 30;
+  for (size_t i = 0; i < pts.size(); ++i) {
+    if (pts[i].second < last_c || (pts[i].second == last_c && pts[i].first == last_e)) {
+      ++pareto;
+      last_e = pts[i].first;
+      last_c = pts[i].second;
+    }
+  }
+  st->best_error = best;
+  st->best_complexity = best_c;
+  st->mean_error = n ? sum / n : 0;
+  st->pareto_size = pareto;
+}
+
+template <class F>
+void for_each_deme(grn_evolution *evo, F &&f) {
+  const int nd = (int)evo->demes.size();
+  int nt = evo->p.n_host_threads > 0 ? evo->p.n_host_threads
+                                     : (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = std::min(nt, nd);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t)
+    pool.emplace_back([&, t]() {
+      for (int d = t; d < nd; d += nt) f(d);
+    });
+  for (int d = 0; d < nd; d += nt) f(d);
+  for (auto &th : pool) th.join();
+}
+
+// SearchAlgoDetCrowd::reproduce (searchalgodetcrowd.cpp:63-101).
+void reproduce(grn_evolution *evo, Deme &d) {
+  d.rng.shuffle(d.perm);
+  d.children.clear();
+  const int n = (int)d.pop.size();
+  for (int i = 0; i + 1 < n; i += 2) {
+    const Individual &p1 = d.pop[d.perm[i]], &p2 = d.pop[d.perm[i + 1]];
+    Individual c1, c2;
+    if (d.rng.rand100() < 75) {
+      evo->ops.cross(d.rng, p1.model, p2.model, &c1.model, &c2.model);
+    } else {
+      c1.model = p1.model;
+      c2.model = p2.model;
+    }
+    evo->ops.mutate(d.rng, d.labels, &c1.model);
+    evo->ops.mutate(d.rng, d.labels, &c2.model);
+    c1.parent_error = p1.error;
+    c2.parent_error = p2.error;
+    c1.complexity = evo->ops.complexity_in_use(c1.model);
+    c2.complexity = evo->ops.complexity_in_use(c2.model);
+    d.children.push_back(std::move(c1));
+    d.children.push_back(std::move(c2));
+  }
+}
+
+// SearchAlgoDetCrowd::chooseNextGeneration (searchalgodetcrowd.cpp:103-147):
+// each child replaces its paired parent if its error is not larger.
+void choose_next(Deme &d) {
+  std::vector<Individual> next;
+  next.reserve(d.pop.size());
+  const int n = (int)d.pop.size();
+  for (int i = 0; i + 1 < n; i += 2) {
+    Individual &p1 = d.pop[d.perm[i]], &p2 = d.pop[d.perm[i + 1]];
+    Individual &c1 = d.children[i], &c2 = d.children[i + 1];
+    next.push_back(c1.error <= p1.error ? std::move(c1) : std::move(p1));
+    next.push_back(c2.error <= p2.error ? std::move(c2) : std::move(p2));
+  }
+  d.pop = std::move(next);
+  d.children.clear();
+}
+
+// Search::createMigrationPartners + migrateIndividuals (search.cpp:263-311).
+void migrate(grn_evolution *evo) {
+  const int nd = (int)evo->demes.size();
+  std::vector<int> ids(nd);
+  for (int i = 0; i < nd; ++i) ids[i] = i;
+  evo->search_rng.shuffle(ids);
+  for (int i = 0; i + 1 < nd; i += 2) {
+    Deme &a = evo->demes[ids[i]], &b = evo->demes[ids[i + 1]];
+    const int n = (int)a.pop.size();
+    std::vector<int> r(2 * n);
+    for (int k = 0; k < 2 * n; ++k) r[k] = k;
+    evo->search_rng.shuffle(r);
+    std::vector<Individual> all;
+    all.reserve(2 * n);
+    for (auto &x : a.pop) all.push_back(std::move(x));
+    for (auto &x : b.pop) all.push_back(std::move(x));
+    a.pop.clear();
+    b.pop.clear();
+    for (int k = 0; k < n; ++k) a.pop.push_back(std::move(all[r[k]]));
+    for (int k = n; k < 2 * n; ++k) b.pop.push_back(std::move(all[r[k]]));
+  }
+}
+
+grn_status gpu_calculator(void *user, const grn_model_batch *batch, const double *max_error,
+                          double *error_out) {
+  return grn_evaluate_batch(static_cast<grn_ctx *>(user), batch, max_error, error_out, nullptr,
+                            nullptr);
+}
+
+double ms_since(std::chrono::steady_clock::time_point t) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+grn_status grn_evolution_create_cb(const grn_evolution_params *params, int n_morphogens,
+                                   grn_error_calculator_fn fn, void *user, grn_evolution **out) {
+  if (!params || !fn || !out || params->n_demes < 1 || params->deme_size < 2 ||
+      n_morphogens < 1 || params->migration_period < 0)
+    return GRN_ERR_INVALID_ARGUMENT;
+  grn_evolution *evo = new (std::nothrow) grn_evolution();
+  if (!evo) return GRN_ERR_OUT_OF_MEMORY;
+  evo->p = *params;
+  evo->ops.n_morph = n_morphogens;
+  evo->ops.n_max_prods = params->n_max_products;
+  evo->ops.n_max_links = params->n_max_links;
+  evo->fn = fn;
+  evo->user = user;
+  evo->search_rng = grn::Rng(params->seed * 0x9E3779B97F4A7C15ull + 0x1234567ull);
+  const int pop = params->deme_size + (params->deme_size % 2);  // even, as the reference
+  evo->demes.resize(params->n_demes);
+  for (int d = 0; d < params->n_demes; ++d) {
+    Deme &dm = evo->demes[d];
+    dm.rng = grn::Rng(params->seed + 0x51ED27ull * (uint64_t)(d + 1));
+    dm.labels = grn::LabelSource{11 + d, params->n_demes};
+    dm.perm.resize(pop);
+    for (int i = 0; i < pop; ++i) dm.perm[i] = i;
+    dm.pop.resize(pop);
+  }
+  *out = evo;
+  return GRN_OK;
+}
+
+grn_status grn_evolution_create(const grn_evolution_params *params, int n_morphogens,
+                                grn_ctx *ctx, grn_evolution **out) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  return grn_evolution_create_cb(params, n_morphogens, gpu_calculator, ctx, out);
+}
+
+grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
+  if (!evo) return GRN_ERR_INVALID_ARGUMENT;
+  grn_generation_stats st{};
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<Individual *> todo;
+  if (evo->generation < 0) {
+    // SearchAlgoDetCrowd::calcInitialPopulation: random models with
+    // nMinProducts = nMorphogens products (searchalgodetcrowd.cpp:54-61).
+    for_each_deme(evo, [&](int d) {
+      Deme &dm = evo->demes[d];
+      for (auto &ind : dm.pop) {
+        ind.model = evo->ops.create_random(dm.rng, evo->ops.n_morph);
+        ind.parent_error = 1000;
+        ind.complexity = evo->ops.complexity_in_use(ind.model);
+      }
+    });
+    for (auto &d : evo->demes)
+      for (auto &ind : d.pop) todo.push_back(&ind);
+  } else {
+    for_each_deme(evo, [&](int d) { reproduce(evo, evo->demes[d]); });
+    for (auto &d : evo->demes)
+      for (auto &ind : d.children) todo.push_back(&ind);
+  }
+  st.host_ms = ms_since(t0);
+  auto t1 = std::chrono::steady_clock::now();
+  grn_status s = evaluate_all(evo, todo);
+  st.eval_ms = ms_since(t1);
+  if (s != GRN_OK) {
+    evo->last_error = "batch evaluation failed";
+    return s;
+  }
+  auto t2 = std::chrono::steady_clock::now();
+  if (evo->generation >= 0)
+    for (auto &d : evo->demes) choose_next(d);
+  evo->generation += 1;
+  if (evo->p.migration_period > 0 && evo->generation > 0 &&
+      evo->generation % evo->p.migration_period == 0 && evo->demes.size() > 1) {
+    migrate(evo);
+    st.migrated = 1;
+  }
+  st.host_ms += ms_since(t2);
+  st.generation = evo->generation;
+  st.n_evaluated = (int32_t)todo.size();
+  fill_stats(evo, &st);
+  if (stats) *stats = st;
+  return GRN_OK;
+}
+
+grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int index,
+                                    grn_product *products, int max_products, int *n_products,
+                                    grn_link *links, int max_links, int *n_links,
+                                    double *error, int *complexity) {
+  if (!evo || deme < 0 || deme >= (int)evo->demes.size() || index < 0 ||
+      index >= (int)evo->demes[deme].pop.size())
+    return GRN_ERR_INVALID_ARGUMENT;
+  const Individual &ind = evo->demes[deme].pop[index];
+  if (n_products) *n_products = (int)ind.model.prods.size();
+  if (n_links) *n_links = (int)ind.model.links.size();
+  if (error) *error = ind.error;
+  if (complexity) *complexity = ind.complexity;
+  if (products) {
+    if ((int)ind.model.prods.size() > max_products) return GRN_ERR_CAPACITY;
+    std::copy(ind.model.prods.begin(), ind.model.prods.end(), products);
+  }
+  if (links) {
+    if ((int)ind.model.links.size() > max_links) return GRN_ERR_CAPACITY;
+    std::copy(ind.model.links.begin(), ind.model.links.end(), links);
+  }
+  return GRN_OK;
+}
+
+grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index) {
+  if (!evo || !deme || !index || evo->generation < 0) return GRN_ERR_INVALID_ARGUMENT;
+  double best = 1e300;
+  int best_c = 1 << 30;
+  for (int d = 0; d < (int)evo->demes.size(); ++d)
+    for (int i = 0; i < (int)evo->demes[d].pop.size(); ++i) {
+      const Individual &ind = evo->demes[d].pop[i];
+      if (ind.error < best || (ind.error == best && ind.complexity < best_c)) {
+        best = ind.error;
+        best_c = ind.complexity;
+        *deme = d;
+        *index = i;
+      }
+    }
+  return GRN_OK;
+}
+
+grn_status grn_evolution_destroy(grn_evolution *evo) {
+  delete evo;
+  return GRN_OK;
+}
+
+}  // extern "C"

@@ -306,6 +306,68 @@ grn_status grn_describe_model(const grn_product *products, int n_products,
                               const grn_link *links, int n_links,
                               int n_morphogens, char *buf, int buf_len);
 
+/* ------------------------------------------------- island evolution ---
+ * Deterministic-crowding island search over GRN models, the reference's
+ * Search + SearchAlgoDetCrowd (Src/Search/search.cpp:101-311,
+ * Src/Search/searchalgodetcrowd.cpp:54-147) with its model operators
+ * (crossover, mutation, excess removal: Src/Model/model.cpp), run
+ * synchronously: every generation all demes reproduce on host threads, all
+ * children are evaluated in one batch, each child replaces its paired parent
+ * if its error is not larger, and every migration_period generations random
+ * deme pairs shuffle their populations together.  Random initial models
+ * have the morphogen products only (nMinProducts = nMorphogens). */
+typedef struct grn_evolution_params {
+  int32_t n_demes;           /* SearchParams::nDemes                       */
+  int32_t deme_size;         /* SearchParams::demesSize (rounded up to even) */
+  int32_t migration_period;  /* SearchParams::migrationPeriod (0: never)   */
+  int32_t n_max_products;    /* SimParams::nMaxProducts in use (-1: any)   */
+  int32_t n_max_links;       /* SimParams::nMaxLinks in use (-1: any)      */
+  int32_t n_host_threads;    /* crossover/mutation threads (0: all cores)  */
+  uint64_t seed;
+} grn_evolution_params;
+
+typedef struct grn_generation_stats {
+  int32_t generation;        /* 0: the evaluated random populations        */
+  int32_t n_evaluated;       /* models evaluated in this generation        */
+  double best_error;         /* lowest error of the populations            */
+  int32_t best_complexity;   /* complexity in use of that model            */
+  int32_t pareto_size;       /* non-dominated (error, complexity) points   */
+  double mean_error;
+  double host_ms;            /* reproduction, selection, migration         */
+  double eval_ms;            /* batch evaluation, wall clock               */
+  int32_t migrated;          /* demes exchanged individuals after it       */
+  int32_t reserved0;
+} grn_generation_stats;
+
+/* A batch fitness evaluator: writes the rounded error (100 above
+ * max_error[m]) of every model, as ErrorCalculator does
+ * (Src/Search/errorcalculator.h:13-21). */
+typedef grn_status (*grn_error_calculator_fn)(void *user, const grn_model_batch *batch,
+                                              const double *max_error, double *error_out);
+
+typedef struct grn_evolution grn_evolution;
+
+/* A search evaluated on this library's GPU evaluator (ctx must have its
+ * experiments uploaded and outlive the search). */
+grn_status grn_evolution_create(const grn_evolution_params *params, int n_morphogens,
+                                grn_ctx *ctx, grn_evolution **out);
+/* A search evaluated by any batch evaluator. */
+grn_status grn_evolution_create_cb(const grn_evolution_params *params, int n_morphogens,
+                                   grn_error_calculator_fn fn, void *user,
+                                   grn_evolution **out);
+/* Runs one generation (the first call creates and evaluates the random
+ * populations). */
+grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats);
+/* Model, error and complexity of individual `index` of deme `deme`
+ * (products/links may be NULL to query the sizes). */
+grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int index,
+                                    grn_product *products, int max_products,
+                                    int *n_products, grn_link *links, int max_links,
+                                    int *n_links, double *error, int *complexity);
+/* Position of the best individual (lowest error, then lowest complexity). */
+grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index);
+grn_status grn_evolution_destroy(grn_evolution *evo);
+
 /* ------------------------------------------------ no-allocation entry ---
  * Device memory that grn_evaluate_batch_noalloc uses instead of allocating:
  * reserved once on every GPU that loads the library and held until the

@@ -1,0 +1,131 @@
+"""Island evolution host (grn_evolution_*): model-operator invariants,
+determinism and deterministic-crowding selection, driven on the CPU by the
+FP64 oracle as the batch evaluator, and on the GPU by the library's own
+evaluator."""
+import numpy as np
+import pytest
+
+import binding as oracle
+import grn_b200 as grn
+import synth
+
+SIM = dict(dim_x=8, dim_y=8, n_input_morphogens=1, n_target_morphogens=1, num_sim_steps=25,
+           error_precision=6, fitness_kind=0, dt=0.1, min_conc=0.0, min_conc_change=1e-3,
+           dist_error_threshold=0.05)
+EVO = dict(n_demes=4, deme_size=10, migration_period=2, n_max_products=6, n_max_links=10,
+           n_host_threads=2, seed=7)
+
+
+def _experiments(sim, seed=3):
+    wl = dict(synth.WORKLOADS["uneven_64x64"], W=sim["dim_x"], H=sim["dim_y"], n_exp=2)
+    return synth.experiments(wl, seed)
+
+
+class OracleCalculator:
+    def __init__(self, sim):
+        self.sim = sim
+        self.init, self.tgt = _experiments(sim)
+        self.calls = []
+
+    def __call__(self, batch, max_error):
+        self.calls.append((batch.n_models, max_error.copy()))
+        err, _, _ = oracle.evaluate_batch(self.sim, self.init, self.tgt, batch, max_error,
+                                          n_threads=2)
+        return err
+
+
+def _check_model(prods, links, n_morph, max_prods, max_links):
+    labels = set(prods["label"].tolist())
+    assert set(range(n_morph)) <= labels  # morphogens are never removed
+    for l in links:
+        assert l["regulator"] in labels and l["regulated"] in labels
+    in_use = oracle.labels_in_use(prods, links, n_morph)
+    assert len(in_use) <= max_prods
+    used = [l for l in links if l["regulator"] in in_use and l["regulated"] in in_use]
+    assert len(used) <= max_links
+    assert all((l["hill_coef"] >= 0) or l["is_and"] for l in links)  # repressors are AND
+
+
+def test_evolution_invariants_with_oracle(built_libs):
+    calc = OracleCalculator(SIM)
+    evo = grn.Evolution(EVO, 2, calculator=calc)
+    stats = [evo.step() for _ in range(6)]
+    assert stats[0]["generation"] == 0 and stats[0]["n_evaluated"] == 40
+    assert all(s["n_evaluated"] == 40 for s in stats)
+    # the global best never gets worse (children replace parents only if not worse)
+    best = [s["best_error"] for s in stats]
+    assert all(b2 <= b1 for b1, b2 in zip(best, best[1:]))
+    assert [s["migrated"] for s in stats] == [0, 0, 1, 0, 1, 0]
+    # initial individuals are evaluated with maxError 1000, children with their parent's error
+    assert (calc.calls[0][1] == 1000.0).all()
+    assert (calc.calls[1][1] <= 1000.0).all() and (calc.calls[1][1] < 1000.0).any()
+    for d in range(4):
+        for i in range(10):
+            prods, links, err, comp = evo.individual(d, i)
+            _check_model(prods, links, 2, EVO["n_max_products"], EVO["n_max_links"])
+            # stored errors are the evaluator's (re-evaluate with maxError 1000)
+            e, _, _ = oracle.evaluate_batch(SIM, calc.init, calc.tgt,
+                                            grn.ModelBatch.from_models([(prods, links)]),
+                                            [1000.0], n_threads=1)
+            assert e[0] == err or err == 100.0
+    d, i = evo.best()
+    assert evo.individual(d, i)[2] == best[-1]
+    evo.close()
+
+
+def test_evolution_is_deterministic(built_libs):
+    runs = []
+    for _ in range(2):
+        calc = OracleCalculator(SIM)
+        evo = grn.Evolution(dict(EVO, seed=11), 2, calculator=calc)
+        st = [evo.step() for _ in range(4)]
+        models = [evo.individual(d, i) for d in range(4) for i in range(10)]
+        runs.append((st, models))
+        evo.close()
+    (s1, m1), (s2, m2) = runs
+    assert [x["best_error"] for x in s1] == [x["best_error"] for x in s2]
+    for a, b in zip(m1, m2):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+
+
+def test_evolution_models_grow_within_limits(built_libs):
+    """Duplication mutations add products; excess removal keeps the
+    products and links in use within the limits."""
+    rng_err = np.random.default_rng(0)
+    evo = grn.Evolution(dict(EVO, deme_size=16, n_max_products=4, n_max_links=5, seed=3), 2,
+                        calculator=lambda b, me: rng_err.random(b.n_models))
+    for _ in range(30):
+        evo.step()
+    sizes = []
+    for d in range(4):
+        for i in range(16):
+            prods, links, _, _ = evo.individual(d, i)
+            _check_model(prods, links, 2, 4, 5)
+            sizes.append(len(prods))
+    assert max(sizes) > 2
+    evo.close()
+
+
+@pytest.mark.gpu
+def test_evolution_on_gpu_matches_oracle_errors():
+    sim = dict(SIM, dim_x=16, dim_y=16, num_sim_steps=60)
+    init, tgt = _experiments(sim)
+    with grn.Evaluator(sim) as ev:
+        ev.set_experiments(init, tgt)
+        evo = grn.Evolution(dict(EVO, deme_size=32, n_max_products=8, n_max_links=24), 2,
+                            evaluator=ev)
+        stats = [evo.step() for _ in range(5)]
+        best = [s["best_error"] for s in stats]
+        assert all(b2 <= b1 for b1, b2 in zip(best, best[1:]))
+        models, errs = [], []
+        for d in range(4):
+            for i in range(0, 32, 4):
+                prods, links, err, _ = evo.individual(d, i)
+                models.append((prods, links))
+                errs.append(err)
+        evo.close()
+    batch = grn.ModelBatch.from_models(models)
+    oe, oraw, _ = oracle.evaluate_batch(sim, init, tgt, batch)
+    errs = np.array(errs)
+    ok = (np.abs(errs - oe) <= 1e-7 + 1e-4 * np.abs(oe)) | (errs == 100.0)
+    assert ok.all(), (errs[~ok], oe[~ok])
