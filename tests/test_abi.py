@@ -20,6 +20,7 @@ HEADER = os.path.join(ROOT, "include", "grn_gpu.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = "\n".join(l for l in text.splitlines() if not l.lstrip().startswith("typedef"))
     return sorted(set(re.findall(r"^[A-Za-z_][\w \*]*?\b(grn_\w+)\s*\(", text, flags=re.M)))
 
 
