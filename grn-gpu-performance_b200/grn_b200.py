@@ -61,7 +61,9 @@ class GenerationStats(ctypes.Structure):
                 ("best_error", ctypes.c_double), ("best_complexity", ctypes.c_int32),
                 ("pareto_size", ctypes.c_int32), ("mean_error", ctypes.c_double),
                 ("host_ms", ctypes.c_double), ("eval_ms", ctypes.c_double),
-                ("migrated", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
+                ("migrated", ctypes.c_int32), ("n_screened", ctypes.c_int32),
+                ("surrogate_ms", ctypes.c_double), ("surrogate_loss", ctypes.c_double),
+                ("n_clones", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
@@ -128,6 +130,19 @@ _SIGNATURES = {
                                   ctypes.POINTER(_I), ctypes.POINTER(_D), ctypes.POINTER(_I)], _I),
     "grn_evolution_best": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "grn_evolution_destroy": ([_P], _I),
+    "grn_encode_models": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
+    "grn_surrogate_create": ([_I, ctypes.c_uint64, _I, ctypes.POINTER(_P)], _I),
+    "grn_surrogate_destroy": ([_P], _I),
+    "grn_surrogate_add_data": ([_P, _P, _P, _I], _I),
+    "grn_surrogate_data_count": ([_P], _I),
+    "grn_surrogate_train": ([_P, _I, _I, ctypes.c_float, ctypes.POINTER(_D)], _I),
+    "grn_surrogate_train_batches": ([_P, _I, _I, ctypes.c_float, ctypes.POINTER(_D)], _I),
+    "grn_surrogate_predict": ([_P, _P, _I, _P], _I),
+    "grn_surrogate_params": ([_P, _P, _I], _I),
+    "grn_surrogate_set_params": ([_P, _P, _I], _I),
+    "grn_surrogate_gradients": ([_P, _P, _P, _I, _P, ctypes.POINTER(_D)], _I),
+    "grn_evolution_set_skip_clones": ([_P, _I], _I),
+    "grn_evolution_set_surrogate": ([_P, _P, _D, _I, _I, _I, ctypes.c_float], _I),
     "grn_evaluate_batch_noalloc": ([ctypes.POINTER(SimParams), _I, _P, _P,
                                     ctypes.POINTER(ModelBatchC), _P, _P, _P, _P,
                                     ctypes.c_char_p, _I], _I),
@@ -459,6 +474,16 @@ class Evolution:
                                                  None, None))
         return prods, links, err.value, c.value
 
+    def set_skip_clones(self, enable=True):
+        _check(self.lib.grn_evolution_set_skip_clones(self.handle, int(bool(enable))))
+
+    def set_surrogate(self, surrogate, simulate_fraction=0.25, min_train_pairs=2048,
+                      batches_per_generation=32, batch_size=512, lr=1e-3):
+        self._sur = surrogate
+        _check(self.lib.grn_evolution_set_surrogate(
+            self.handle, surrogate.handle if surrogate else None, simulate_fraction,
+            min_train_pairs, batches_per_generation, batch_size, lr))
+
     def best(self):
         d, i = ctypes.c_int(), ctypes.c_int()
         _check(self.lib.grn_evolution_best(self.handle, ctypes.byref(d), ctypes.byref(i)))
@@ -467,6 +492,84 @@ class Evolution:
     def close(self):
         if self.handle:
             self.lib.grn_evolution_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+N_FEATURES = 128
+N_PARAMS = 164865
+
+
+def encode_models(batch, n_morphogens):
+    """grn_encode_models: [n][128] float32 encodings (host only)."""
+    out = np.zeros((batch.n_models, N_FEATURES), np.float32)
+    cb = batch.as_c()
+    _check(load_library().grn_encode_models(ctypes.byref(cb), n_morphogens, _ptr(out)))
+    return out
+
+
+class Surrogate:
+    """The surrogate MLP (grn_surrogate_*)."""
+
+    def __init__(self, device=0, seed=0, capacity=200000):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self.lib.grn_surrogate_create(device, seed, capacity, ctypes.byref(h)))
+        self.handle = h
+
+    def add_data(self, features, log_error):
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(log_error, np.float32)
+        _check(self.lib.grn_surrogate_add_data(self.handle, _ptr(f), _ptr(t), len(t)))
+
+    @property
+    def data_count(self):
+        return self.lib.grn_surrogate_data_count(self.handle)
+
+    def train(self, epochs=1, batch_size=512, lr=1e-3):
+        loss = ctypes.c_double()
+        _check(self.lib.grn_surrogate_train(self.handle, epochs, batch_size, lr,
+                                            ctypes.byref(loss)))
+        return loss.value
+
+    def train_batches(self, n_batches, batch_size=512, lr=1e-3):
+        loss = ctypes.c_double()
+        _check(self.lib.grn_surrogate_train_batches(self.handle, n_batches, batch_size, lr,
+                                                    ctypes.byref(loss)))
+        return loss.value
+
+    def predict(self, features):
+        f = np.ascontiguousarray(features, np.float32)
+        out = np.zeros(len(f), np.float32)
+        _check(self.lib.grn_surrogate_predict(self.handle, _ptr(f), len(f), _ptr(out)))
+        return out
+
+    def params(self):
+        out = np.zeros(N_PARAMS, np.float32)
+        _check(self.lib.grn_surrogate_params(self.handle, _ptr(out), N_PARAMS))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(self.lib.grn_surrogate_set_params(self.handle, _ptr(p), N_PARAMS))
+
+    def gradients(self, features, log_error):
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(log_error, np.float32)
+        g = np.zeros(N_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        _check(self.lib.grn_surrogate_gradients(self.handle, _ptr(f), _ptr(t), len(t), _ptr(g),
+                                                ctypes.byref(loss)))
+        return loss.value, g
+
+    def close(self):
+        if self.handle:
+            self.lib.grn_surrogate_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

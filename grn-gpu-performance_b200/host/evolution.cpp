@@ -324,6 +324,7 @@ struct Individual {
   double error = -1;
   double parent_error = 1000;  // Individual.cpp:19-25: random individuals
   int complexity = 0;
+  bool clone = false;  // same simulated program as its paired parent
 };
 
 struct Deme {
@@ -341,6 +342,12 @@ struct grn_evolution {
   grn::ModelOps ops{};
   grn_error_calculator_fn fn = nullptr;
   void *user = nullptr;
+  grn_ctx *ctx = nullptr;  // GPU evaluator (raw errors available), or null
+  grn_surrogate *sur = nullptr;
+  bool skip_clones = false;
+  double sim_fraction = 0.25;
+  int min_train = 2048, batches = 32, batch = 512;
+  float lr = 1e-3f;
   std::vector<Deme> demes;
   grn::Rng search_rng{0};
   int generation = -1;
@@ -349,27 +356,110 @@ struct grn_evolution {
 
 namespace {
 
-grn_status evaluate_all(grn_evolution *evo, std::vector<Individual *> &inds) {
-  std::vector<int32_t> po(1, 0), lo(1, 0);
+// Models of `inds` as one grn_model_batch (views into the vectors).
+struct FlatBatch {
+  std::vector<int32_t> po{0}, lo{0};
   std::vector<grn_product> prods;
   std::vector<grn_link> links;
-  std::vector<double> max_err, err(inds.size());
-  for (Individual *ind : inds) {
-    prods.insert(prods.end(), ind->model.prods.begin(), ind->model.prods.end());
-    links.insert(links.end(), ind->model.links.begin(), ind->model.links.end());
-    po.push_back((int32_t)prods.size());
-    lo.push_back((int32_t)links.size());
-    max_err.push_back(ind->parent_error);
-  }
   grn_model_batch b{};
-  b.n_models = (int32_t)inds.size();
-  b.product_offsets = po.data();
-  b.products = prods.empty() ? nullptr : prods.data();
-  b.link_offsets = lo.data();
-  b.links = links.empty() ? nullptr : links.data();
-  const grn_status s = evo->fn(evo->user, &b, max_err.data(), err.data());
+  explicit FlatBatch(const std::vector<Individual *> &inds) {
+    for (Individual *ind : inds) {
+      prods.insert(prods.end(), ind->model.prods.begin(), ind->model.prods.end());
+      links.insert(links.end(), ind->model.links.begin(), ind->model.links.end());
+      po.push_back((int32_t)prods.size());
+      lo.push_back((int32_t)links.size());
+    }
+    b.n_models = (int32_t)inds.size();
+    b.product_offsets = po.data();
+    b.products = prods.empty() ? nullptr : prods.data();
+    b.link_offsets = lo.data();
+    b.links = links.empty() ? nullptr : links.data();
+  }
+};
+
+// Evaluates `inds` with max error = their parent's error.  raw_out gets the
+// unrounded errors when the GPU evaluator is used, else the rounded ones.
+grn_status evaluate_all(grn_evolution *evo, std::vector<Individual *> &inds,
+                        std::vector<double> *raw_out) {
+  FlatBatch fb(inds);
+  std::vector<double> max_err, err(inds.size()), raw(inds.size());
+  for (Individual *ind : inds) max_err.push_back(ind->parent_error);
+  grn_status s;
+  if (evo->ctx)
+    s = grn_evaluate_batch(evo->ctx, &fb.b, max_err.data(), err.data(), raw.data(), nullptr);
+  else
+    s = evo->fn(evo->user, &fb.b, max_err.data(), err.data());
   if (s != GRN_OK) return s;
   for (size_t i = 0; i < inds.size(); ++i) inds[i]->error = err[i];
+  if (raw_out) *raw_out = evo->ctx ? raw : err;
+  return GRN_OK;
+}
+
+// What the simulation of a model reads, in FP64: the first product of every
+// label in use (ascending), then every link whose regulated label is in use,
+// in model order.  Models with equal keys have equal errors under any
+// deterministic evaluator.
+std::vector<double> program_key(const GModel &m, int n_morph) {
+  const std::vector<int> in_use = grn::labels_in_use(m, n_morph);
+  std::vector<double> k;
+  for (int label : in_use) {
+    const grn_product *p = nullptr;
+    for (const auto &q : m.prods)
+      if (q.label == label) {
+        p = &q;
+        break;
+      }
+    k.push_back(label);
+    if (p) {
+      k.push_back(p->lim);
+      k.push_back(p->deg);
+      k.push_back(p->dif);
+    } else {
+      k.push_back(std::nan(""));  // never equal: the evaluator reports the error
+    }
+  }
+  for (const auto &l : m.links)
+    if (std::binary_search(in_use.begin(), in_use.end(), l.regulated)) {
+      k.push_back(l.regulator);
+      k.push_back(l.regulated);
+      k.push_back(l.dis_const);
+      k.push_back(l.hill_coef);
+      k.push_back(l.is_and != 0);
+    }
+  return k;
+}
+
+bool same_key(const std::vector<double> &a, const std::vector<double> &b) {
+  return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(double)) == 0 &&
+         std::all_of(a.begin(), a.end(), [](double x) { return x == x; });
+}
+
+// Adds simulated pairs to the surrogate's training set and trains it.  A
+// simulation abandoned past the parent's error leaves a lower bound (the raw
+// error reached so far, or the parent's error behind the rounded 100 of a
+// callback evaluator); it is kept as the target, so that the set is not
+// biased towards children that beat their parents.
+grn_status feed_surrogate(grn_evolution *evo, const std::vector<Individual *> &inds,
+                          const std::vector<double> &raw, grn_generation_stats *st) {
+  std::vector<Individual *> keep;
+  std::vector<float> target;
+  for (size_t i = 0; i < inds.size(); ++i) {
+    double r = raw[i];
+    if (!evo->ctx && r == 100.0 && inds[i]->parent_error < 100.0) r = inds[i]->parent_error;
+    if (!(r > 0) || !std::isfinite(r)) continue;
+    keep.push_back(inds[i]);
+    target.push_back((float)std::log(r));
+  }
+  if (!keep.empty()) {
+    FlatBatch fb(keep);
+    std::vector<float> feat((size_t)keep.size() * GRN_SURROGATE_FEATURES);
+    grn_status s = grn_encode_models(&fb.b, evo->ops.n_morph, feat.data());
+    if (s == GRN_OK) s = grn_surrogate_add_data(evo->sur, feat.data(), target.data(), (int)keep.size());
+    if (s != GRN_OK) return s;
+  }
+  if (grn_surrogate_data_count(evo->sur) > 0 && evo->batches > 0)
+    return grn_surrogate_train_batches(evo->sur, evo->batches, evo->batch, evo->lr,
+                                       &st->surrogate_loss);
   return GRN_OK;
 }
 
@@ -531,7 +621,30 @@ grn_status grn_evolution_create_cb(const grn_evolution_params *params, int n_mor
 grn_status grn_evolution_create(const grn_evolution_params *params, int n_morphogens,
                                 grn_ctx *ctx, grn_evolution **out) {
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
-  return grn_evolution_create_cb(params, n_morphogens, gpu_calculator, ctx, out);
+  grn_status s = grn_evolution_create_cb(params, n_morphogens, gpu_calculator, ctx, out);
+  if (s == GRN_OK) (*out)->ctx = ctx;
+  return s;
+}
+
+grn_status grn_evolution_set_skip_clones(grn_evolution *evo, int enable) {
+  if (!evo) return GRN_ERR_INVALID_ARGUMENT;
+  evo->skip_clones = enable != 0;
+  return GRN_OK;
+}
+
+grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
+                                       double simulate_fraction, int min_train_pairs,
+                                       int batches_per_generation, int batch_size, float lr) {
+  if (!evo || (s && (!(simulate_fraction > 0) || simulate_fraction > 1 || min_train_pairs < 1 ||
+                     batches_per_generation < 0 || batch_size < 1 || !(lr > 0))))
+    return GRN_ERR_INVALID_ARGUMENT;
+  evo->sur = s;
+  evo->sim_fraction = simulate_fraction;
+  evo->min_train = min_train_pairs;
+  evo->batches = batches_per_generation;
+  evo->batch = batch_size;
+  evo->lr = lr;
+  return GRN_OK;
 }
 
 grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
@@ -553,17 +666,67 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
     for (auto &d : evo->demes)
       for (auto &ind : d.pop) todo.push_back(&ind);
   } else {
-    for_each_deme(evo, [&](int d) { reproduce(evo, evo->demes[d]); });
+    for_each_deme(evo, [&](int d) {
+      Deme &dm = evo->demes[d];
+      reproduce(evo, dm);
+      if (!(evo->skip_clones || evo->sur)) return;
+      // A child whose simulated program equals its paired parent's has the
+      // parent's error: accept it without simulating (neutral drift kept).
+      for (size_t i = 0; i < dm.children.size(); ++i) {
+        Individual &c = dm.children[i];
+        const Individual &p = dm.pop[dm.perm[i]];
+        c.clone = p.error < 100 && same_key(program_key(c.model, evo->ops.n_morph),
+                                            program_key(p.model, evo->ops.n_morph));
+        if (c.clone) c.error = p.error;
+      }
+    });
     for (auto &d : evo->demes)
-      for (auto &ind : d.children) todo.push_back(&ind);
+      for (auto &ind : d.children) {
+        if (ind.clone) st.n_clones += 1;
+        else todo.push_back(&ind);
+      }
   }
   st.host_ms = ms_since(t0);
+  // Surrogate screening: simulate only the most promising children.
+  std::vector<Individual *> sim = todo;
+  if (evo->sur && evo->generation >= 0 &&
+      grn_surrogate_data_count(evo->sur) >= evo->min_train) {
+    auto ts = std::chrono::steady_clock::now();
+    FlatBatch fb(todo);
+    std::vector<float> feat((size_t)todo.size() * GRN_SURROGATE_FEATURES), pred(todo.size());
+    grn_status s = grn_encode_models(&fb.b, evo->ops.n_morph, feat.data());
+    if (s == GRN_OK) s = grn_surrogate_predict(evo->sur, feat.data(), (int)todo.size(), pred.data());
+    if (s != GRN_OK) return s;
+    std::vector<int> order(todo.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    auto score = [&](int i) {
+      return (double)pred[i] - std::log(std::max(todo[i]->parent_error, 1e-30));
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score(a) < score(b); });
+    const size_t n_sim = std::max<size_t>(1, (size_t)std::ceil(evo->sim_fraction * todo.size()));
+    sim.clear();
+    std::vector<char> chosen(todo.size(), 0);
+    for (size_t k = 0; k < n_sim && k < order.size(); ++k) chosen[order[k]] = 1;
+    for (size_t i = 0; i < todo.size(); ++i) {
+      if (chosen[i]) sim.push_back(todo[i]);
+      else todo[i]->error = HUGE_VAL;  // not simulated: its parent stays
+    }
+    st.n_screened = (int32_t)todo.size();
+    st.surrogate_ms += ms_since(ts);
+  }
   auto t1 = std::chrono::steady_clock::now();
-  grn_status s = evaluate_all(evo, todo);
+  std::vector<double> raw;
+  grn_status s = evaluate_all(evo, sim, &raw);
   st.eval_ms = ms_since(t1);
   if (s != GRN_OK) {
     evo->last_error = "batch evaluation failed";
     return s;
+  }
+  if (evo->sur) {
+    auto ts = std::chrono::steady_clock::now();
+    s = feed_surrogate(evo, sim, raw, &st);
+    st.surrogate_ms += ms_since(ts);
+    if (s != GRN_OK) return s;
   }
   auto t2 = std::chrono::steady_clock::now();
   if (evo->generation >= 0)
@@ -576,7 +739,7 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
   }
   st.host_ms += ms_since(t2);
   st.generation = evo->generation;
-  st.n_evaluated = (int32_t)todo.size();
+  st.n_evaluated = (int32_t)sim.size();
   fill_stats(evo, &st);
   if (stats) *stats = st;
   return GRN_OK;

@@ -1,0 +1,367 @@
+// surrogate.cpp -- surrogate fitness model: encoding of GRN models, and the
+// host side of training and inference of a 128-256-256-256-1 ReLU MLP whose
+// GEMMs run on the tensor cores (csrc/grn_mlp.cu).  It predicts log(error)
+// of a model from its compiled program so that the island search can
+// simulate only the most promising offspring.  No reference counterpart.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/grn_gpu.h"
+#include "../csrc/grn_mlp.h"
+#include "pack.h"
+
+namespace {
+
+constexpr int kF = GRN_SURROGATE_FEATURES;  // 128
+constexpr int kH = GRN_SURROGATE_HIDDEN;    // 256
+// Parameter layout (FP32 master copy; the BF16 mirror has the same layout).
+constexpr int64_t kW1 = 0, kB1 = kW1 + (int64_t)kH * kF;
+constexpr int64_t kW2 = kB1 + kH, kB2 = kW2 + (int64_t)kH * kH;
+constexpr int64_t kW3 = kB2 + kH, kB3 = kW3 + (int64_t)kH * kH;
+constexpr int64_t kW4 = kB3 + kH, kB4 = kW4 + kH;
+constexpr int64_t kP = kB4 + 1;
+static_assert(kP == GRN_SURROGATE_PARAMS, "parameter count");
+
+#define GRN_CK(expr)                                   \
+  do {                                                 \
+    cudaError_t e__ = (expr);                          \
+    if (e__ != cudaSuccess) return GRN_ERR_CUDA;       \
+  } while (0)
+
+}  // namespace
+
+struct grn_surrogate {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+  __nv_bfloat16 *wb = nullptr;
+  int bmax = 0;
+  __nv_bfloat16 *x = nullptr, *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;
+  __nv_bfloat16 *dz1 = nullptr, *dz2 = nullptr, *dz3 = nullptr;
+  float *y = nullptr, *t = nullptr, *dy = nullptr;
+  double *loss = nullptr;
+  int32_t *idx = nullptr;
+  int cap = 0, count = 0, head = 0;  // dataset ring buffer
+  __nv_bfloat16 *dx = nullptr;
+  float *dt = nullptr;
+  int step = 0;
+  std::mt19937_64 rng;
+};
+
+namespace {
+
+grn_status forward(grn_surrogate *s, int B) {
+  using namespace grn;
+  cudaStream_t st = s->st;
+  GRN_CK(mlp_gemm(B, kH, kF, s->x, kF, 1, s->wb + kW1, kF, 1, kEpiBiasRelu, nullptr, s->h1, kH,
+                  s->w + kB1, nullptr, st));
+  GRN_CK(mlp_gemm(B, kH, kH, s->h1, kH, 1, s->wb + kW2, kH, 1, kEpiBiasRelu, nullptr, s->h2, kH,
+                  s->w + kB2, nullptr, st));
+  GRN_CK(mlp_gemm(B, kH, kH, s->h2, kH, 1, s->wb + kW3, kH, 1, kEpiBiasRelu, nullptr, s->h3, kH,
+                  s->w + kB3, nullptr, st));
+  GRN_CK(mlp_output_forward(B, kH, s->h3, s->w + kW4, s->w + kB4, s->y, st));
+  return GRN_OK;
+}
+
+// Loss and gradients of a minibatch already in s->x / s->t (after forward).
+grn_status backward(grn_surrogate *s, int B) {
+  using namespace grn;
+  cudaStream_t st = s->st;
+  GRN_CK(mlp_loss(B, s->y, s->t, s->dy, s->loss, st));
+  GRN_CK(mlp_output_backward(B, kH, s->h3, s->w + kW4, s->dy, s->g + kW4, s->g + kB4, s->dz3,
+                             st));
+  // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * [H2 > 0]
+  GRN_CK(mlp_gemm(kH, kH, B, s->dz3, 1, kH, s->h2, 1, kH, kEpiF32, s->g + kW3, nullptr, kH,
+                  nullptr, nullptr, st));
+  GRN_CK(mlp_column_sum(B, kH, s->dz3, s->g + kB3, st));
+  GRN_CK(mlp_gemm(B, kH, kH, s->dz3, kH, 1, s->wb + kW3, 1, kH, kEpiMask, nullptr, s->dz2, kH,
+                  nullptr, s->h2, st));
+  // layer 2
+  GRN_CK(mlp_gemm(kH, kH, B, s->dz2, 1, kH, s->h1, 1, kH, kEpiF32, s->g + kW2, nullptr, kH,
+                  nullptr, nullptr, st));
+  GRN_CK(mlp_column_sum(B, kH, s->dz2, s->g + kB2, st));
+  GRN_CK(mlp_gemm(B, kH, kH, s->dz2, kH, 1, s->wb + kW2, 1, kH, kEpiMask, nullptr, s->dz1, kH,
+                  nullptr, s->h1, st));
+  // layer 1: dW1 = dZ1^T X (no input gradient needed)
+  GRN_CK(mlp_gemm(kH, kF, B, s->dz1, 1, kH, s->x, 1, kF, kEpiF32, s->g + kW1, nullptr, kF,
+                  nullptr, nullptr, st));
+  GRN_CK(mlp_column_sum(B, kH, s->dz1, s->g + kB1, st));
+  return GRN_OK;
+}
+
+// One Adam step on the training-set rows idx[0..B); adds its loss to *loss_sum.
+grn_status train_minibatch(grn_surrogate *s, const int32_t *idx, int B, float lr,
+                           double *loss_sum) {
+  GRN_CK(cudaMemcpyAsync(s->idx, idx, (size_t)B * 4, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(grn::mlp_gather_rows(B, kF, s->idx, s->dx, s->dt, s->x, s->t, s->st));
+  grn_status st = forward(s, B);
+  if (st == GRN_OK) st = backward(s, B);
+  if (st != GRN_OK) return st;
+  s->step += 1;
+  GRN_CK(grn::mlp_adam((int)kP, s->w, s->g, s->m, s->v, lr, 0.9f, 0.999f, 1e-8f, s->step, s->wb,
+                       s->st));
+  double l = 0;
+  GRN_CK(cudaMemcpyAsync(&l, s->loss, 8, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  *loss_sum += l;
+  return GRN_OK;
+}
+
+grn_status upload_features(grn_surrogate *s, const float *features, int n, __nv_bfloat16 *dst) {
+  std::vector<__nv_bfloat16> hb((size_t)n * kF);
+  for (size_t i = 0; i < hb.size(); ++i) hb[i] = __float2bfloat16(features[i]);
+  GRN_CK(cudaMemcpyAsync(dst, hb.data(), hb.size() * sizeof(__nv_bfloat16),
+                         cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  return GRN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+grn_status grn_encode_models(const grn_model_batch *batch, int n_morphogens, float *features) {
+  if (!batch || !features || batch->n_models < 0 || n_morphogens < 0)
+    return GRN_ERR_INVALID_ARGUMENT;
+  for (int m = 0; m < batch->n_models; ++m) {
+    float *f = features + (size_t)m * kF;
+    std::memset(f, 0, sizeof(float) * kF);
+    const int p0 = batch->product_offsets[m], p1 = batch->product_offsets[m + 1];
+    const int l0 = batch->link_offsets[m], l1 = batch->link_offsets[m + 1];
+    std::vector<uint4> rec;
+    grn::ModelCost cost;
+    std::string err;
+    const grn_status s = grn::pack_model(batch->products + p0, p1 - p0, batch->links + l0,
+                                         l1 - l0, n_morphogens, m, &rec, &cost, &err);
+    if (s != GRN_OK) return s;
+    grn::PackedHeader hdr;
+    std::memcpy(&hdr, rec.data(), sizeof hdr);
+    // 8 genes x (lim, deg, dif, in use), then 24 links x (regulator slot / 8,
+    // K, signed Hill coefficient / 5, +-(regulated gene + 1) / 8 with the sign
+    // - for AND and + for OR), links in program order (each gene's OR links,
+    // then its AND links).  K and n come back from the exponent form
+    // a = -n_signed, b = -a * lg2(K).
+    int li = 0;
+    for (int gi = 0; gi < hdr.n_genes; ++gi) {
+      grn::PackedGene g;
+      std::memcpy(&g, rec.data() + 1 + gi, sizeof g);
+      if (gi < 8) {
+        f[4 * gi + 0] = g.lim;
+        f[4 * gi + 1] = g.deg;
+        f[4 * gi + 2] = g.dif;
+        f[4 * gi + 3] = 1.0f;
+      }
+      for (int l = 0; l < g.n_or + g.n_and && li < 24; ++l, ++li) {
+        grn::PackedLink lk;
+        std::memcpy(&lk, rec.data() + 1 + hdr.n_genes + g.link_begin + l, sizeof lk);
+        float *q = f + 32 + 4 * li;
+        const bool konst = lk.slot == grn::kConstSlot;
+        q[0] = konst ? -0.125f : lk.slot / 8.0f;
+        const float k = (konst || lk.a == 0.0f) ? 0.0f : std::exp2(-lk.b / lk.a);
+        q[1] = std::isfinite(k) ? std::min(k, 4.0f) : 4.0f;
+        q[2] = -lk.a / 5.0f;
+        q[3] = (l < g.n_or ? 1.0f : -1.0f) * (gi + 1) / 8.0f;
+      }
+    }
+  }
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_create(int device, uint64_t seed, int capacity, grn_surrogate **out) {
+  if (!out || capacity < 1) return GRN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) {
+    cudaGetLastError();
+    return GRN_ERR_NO_DEVICE;
+  }
+  grn_surrogate *s = new (std::nothrow) grn_surrogate();
+  if (!s) return GRN_ERR_OUT_OF_MEMORY;
+  s->device = device;
+  s->rng.seed(seed);
+  s->cap = capacity;
+  s->bmax = 8192;
+  cudaSetDevice(device);
+  bool ok = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) == cudaSuccess;
+  auto alloc = [&](void **p, size_t bytes) {
+    if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+  };
+  alloc((void **)&s->w, kP * 4);
+  alloc((void **)&s->g, kP * 4);
+  alloc((void **)&s->m, kP * 4);
+  alloc((void **)&s->v, kP * 4);
+  alloc((void **)&s->wb, kP * 2);
+  const size_t B = s->bmax;
+  alloc((void **)&s->x, B * kF * 2);
+  for (__nv_bfloat16 **p : {&s->h1, &s->h2, &s->h3, &s->dz1, &s->dz2, &s->dz3})
+    alloc((void **)p, B * kH * 2);
+  alloc((void **)&s->y, B * 4);
+  alloc((void **)&s->t, B * 4);
+  alloc((void **)&s->dy, B * 4);
+  alloc((void **)&s->loss, 8);
+  alloc((void **)&s->idx, B * 4);
+  alloc((void **)&s->dx, (size_t)capacity * kF * 2);
+  alloc((void **)&s->dt, (size_t)capacity * 4);
+  if (!ok) {
+    grn_surrogate_destroy(s);
+    return GRN_ERR_OUT_OF_MEMORY;
+  }
+  // He initialisation for the ReLU layers, small output layer, zero biases.
+  std::vector<float> w(kP, 0.0f);
+  auto init = [&](int64_t off, int rows, int fan_in, float scale) {
+    std::normal_distribution<float> nd(0.0f, scale * std::sqrt(2.0f / fan_in));
+    for (int64_t i = 0; i < (int64_t)rows * fan_in; ++i) w[off + i] = nd(s->rng);
+  };
+  init(kW1, kH, kF, 1.0f);
+  init(kW2, kH, kH, 1.0f);
+  init(kW3, kH, kH, 1.0f);
+  init(kW4, 1, kH, 0.5f);
+  w[kB4] = -1.0f;  // typical log(error) of random models
+  if (grn_surrogate_set_params(s, w.data(), (int)kP) != GRN_OK) {
+    grn_surrogate_destroy(s);
+    return GRN_ERR_CUDA;
+  }
+  *out = s;
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_destroy(grn_surrogate *s) {
+  if (!s) return GRN_OK;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  for (void *p : {(void *)s->w, (void *)s->g, (void *)s->m, (void *)s->v, (void *)s->wb,
+                  (void *)s->x, (void *)s->h1, (void *)s->h2, (void *)s->h3, (void *)s->dz1,
+                  (void *)s->dz2, (void *)s->dz3, (void *)s->y, (void *)s->t, (void *)s->dy,
+                  (void *)s->loss, (void *)s->idx, (void *)s->dx, (void *)s->dt})
+    if (p) cudaFree(p);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n) {
+  if (!s || !params || n != kP) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  GRN_CK(cudaMemcpyAsync(s->w, params, kP * 4, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaMemsetAsync(s->m, 0, kP * 4, s->st));
+  GRN_CK(cudaMemsetAsync(s->v, 0, kP * 4, s->st));
+  GRN_CK(grn::mlp_to_bf16((int)kP, s->w, s->wb, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  s->step = 0;
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_params(grn_surrogate *s, float *out, int n) {
+  if (!s || !out || n != kP) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  GRN_CK(cudaMemcpyAsync(out, s->w, kP * 4, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_add_data(grn_surrogate *s, const float *features, const float *log_error,
+                                  int n) {
+  if (!s || n < 0 || (n > 0 && (!features || !log_error))) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  for (int i = 0; i < n;) {
+    const int chunk = std::min(n - i, s->cap - s->head);
+    grn_status st = upload_features(s, features + (size_t)i * kF, chunk,
+                                    s->dx + (size_t)s->head * kF);
+    if (st != GRN_OK) return st;
+    GRN_CK(cudaMemcpyAsync(s->dt + s->head, log_error + i, chunk * 4, cudaMemcpyHostToDevice,
+                           s->st));
+    GRN_CK(cudaStreamSynchronize(s->st));
+    s->head = (s->head + chunk) % s->cap;
+    s->count = std::min(s->cap, s->count + chunk);
+    i += chunk;
+  }
+  return GRN_OK;
+}
+
+int grn_surrogate_data_count(const grn_surrogate *s) { return s ? s->count : 0; }
+
+grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, float lr,
+                               double *mean_loss) {
+  if (!s || epochs < 0 || batch_size < 1 || batch_size > s->bmax || !(lr > 0))
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  std::vector<int32_t> perm(s->count);
+  double loss_sum = 0;
+  long n_batches = 0;
+  for (int e = 0; e < epochs; ++e) {
+    for (int i = 0; i < s->count; ++i) perm[i] = i;
+    std::shuffle(perm.begin(), perm.end(), s->rng);
+    for (int b0 = 0; b0 < s->count; b0 += batch_size) {
+      const int B = std::min(batch_size, s->count - b0);
+      grn_status st = train_minibatch(s, perm.data() + b0, B, lr, &loss_sum);
+      if (st != GRN_OK) return st;
+      ++n_batches;
+    }
+  }
+  if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batch_size, float lr,
+                                       double *mean_loss) {
+  if (!s || n_batches < 0 || batch_size < 1 || batch_size > s->bmax || !(lr > 0))
+    return GRN_ERR_INVALID_ARGUMENT;
+  if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  const int B = std::min(batch_size, s->count);
+  std::vector<int32_t> idx(B);
+  std::uniform_int_distribution<int32_t> pick(0, s->count - 1);
+  double loss_sum = 0;
+  for (int it = 0; it < n_batches; ++it) {
+    for (int i = 0; i < B; ++i) idx[i] = pick(s->rng);
+    grn_status st = train_minibatch(s, idx.data(), B, lr, &loss_sum);
+    if (st != GRN_OK) return st;
+  }
+  if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n, float *out) {
+  if (!s || n < 0 || (n > 0 && (!features || !out))) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  for (int i = 0; i < n; i += s->bmax) {
+    const int B = std::min(s->bmax, n - i);
+    grn_status st = upload_features(s, features + (size_t)i * kF, B, s->x);
+    if (st == GRN_OK) st = forward(s, B);
+    if (st != GRN_OK) return st;
+    GRN_CK(cudaMemcpyAsync(out + i, s->y, B * 4, cudaMemcpyDeviceToHost, s->st));
+    GRN_CK(cudaStreamSynchronize(s->st));
+  }
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
+                                   const float *log_error, int n, float *grads, double *loss) {
+  if (!s || !features || !log_error || !grads || n < 1 || n > s->bmax)
+    return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  grn_status st = upload_features(s, features, n, s->x);
+  if (st != GRN_OK) return st;
+  GRN_CK(cudaMemcpyAsync(s->t, log_error, n * 4, cudaMemcpyHostToDevice, s->st));
+  st = forward(s, n);
+  if (st == GRN_OK) st = backward(s, n);
+  if (st != GRN_OK) return st;
+  GRN_CK(cudaMemcpyAsync(grads, s->g, kP * 4, cudaMemcpyDeviceToHost, s->st));
+  double l = 0;
+  GRN_CK(cudaMemcpyAsync(&l, s->loss, 8, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  if (loss) *loss = l;
+  return GRN_OK;
+}
+
+}  // extern "C"

@@ -336,6 +336,10 @@ typedef struct grn_generation_stats {
   double host_ms;            /* reproduction, selection, migration         */
   double eval_ms;            /* batch evaluation, wall clock               */
   int32_t migrated;          /* demes exchanged individuals after it       */
+  int32_t n_screened;        /* children ranked by the surrogate (else 0)  */
+  double surrogate_ms;       /* encode + predict + train, wall clock       */
+  double surrogate_loss;     /* mean training loss of this generation      */
+  int32_t n_clones;          /* children accepted without simulation       */
   int32_t reserved0;
 } grn_generation_stats;
 
@@ -367,6 +371,68 @@ grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int inde
 /* Position of the best individual (lowest error, then lowest complexity). */
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index);
 grn_status grn_evolution_destroy(grn_evolution *evo);
+
+/* Off by default (the reference simulates every child).  When enabled, a
+ * child whose simulated program -- the products in use and the links into
+ * them, compared bit for bit -- equals its paired parent's takes the
+ * parent's error without being simulated; selection is unchanged, because a
+ * deterministic evaluator would return that same error.  Always on while a
+ * surrogate is attached. */
+grn_status grn_evolution_set_skip_clones(grn_evolution *evo, int enable);
+
+/* ------------------------------------------------------ surrogate MLP ---
+ * A learned fitness model that pre-screens offspring (no reference
+ * counterpart: the reference simulates every child).  A ReLU MLP
+ * 128 -> 256 -> 256 -> 256 -> 1 over a padded encoding of a model's compiled
+ * program predicts log(error); its GEMMs run on the tensor cores with BF16
+ * operands and FP32 accumulation, trained with Adam on (model, error) pairs
+ * the simulator produces. */
+#define GRN_SURROGATE_FEATURES 128
+#define GRN_SURROGATE_HIDDEN 256
+#define GRN_SURROGATE_PARAMS 164865  /* W1 b1 W2 b2 W3 b3 w4 b4, FP32 */
+
+typedef struct grn_surrogate grn_surrogate;
+
+/* Encoding [n_models][128]: products in use 0..7 as (lim, deg, dif, 1), then
+ * up to 24 used links in program order (per regulated product: OR links,
+ * then AND links) as (regulator index / 8 or -1/8 for a constant term,
+ * K clipped to [0, 4], signed Hill coefficient / 5, (regulated index + 1) / 8
+ * signed - for AND and + for OR); zero padding.  Host only. */
+grn_status grn_encode_models(const grn_model_batch *batch, int n_morphogens, float *features);
+
+/* Surrogate on `device` with a training set ring buffer of `capacity` pairs. */
+grn_status grn_surrogate_create(int device, uint64_t seed, int capacity, grn_surrogate **out);
+grn_status grn_surrogate_destroy(grn_surrogate *s);
+/* Appends (encoding, log error) pairs to the training set (oldest dropped
+ * past capacity). */
+grn_status grn_surrogate_add_data(grn_surrogate *s, const float *features,
+                                  const float *log_error, int n);
+int grn_surrogate_data_count(const grn_surrogate *s);
+/* Adam epochs over the training set; mean minibatch loss in *mean_loss. */
+grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, float lr,
+                               double *mean_loss);
+/* n_batches Adam steps on minibatches drawn uniformly from the training set. */
+grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batch_size, float lr,
+                                       double *mean_loss);
+/* Predicted log(error) of n encodings. */
+grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n,
+                                 float *log_error_out);
+/* FP32 parameters (GRN_SURROGATE_PARAMS values) out / in (in resets Adam). */
+grn_status grn_surrogate_params(grn_surrogate *s, float *params, int n);
+grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n);
+/* Mean squared loss and its parameter gradients on n pairs, no update. */
+grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
+                                   const float *log_error, int n, float *grads, double *loss);
+
+/* Screens offspring with a surrogate: once it holds min_train_pairs
+ * simulated pairs, every generation ranks all children by predicted
+ * log(error) minus log(parent error) and simulates only the best
+ * simulate_fraction of them (the others lose to their parents); the
+ * simulated pairs are added to its training set and it takes
+ * batches_per_generation Adam steps.  NULL detaches it. */
+grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
+                                       double simulate_fraction, int min_train_pairs,
+                                       int batches_per_generation, int batch_size, float lr);
 
 /* ------------------------------------------------ no-allocation entry ---
  * Device memory that grn_evaluate_batch_noalloc uses instead of allocating:

@@ -88,6 +88,28 @@ def test_evolution_is_deterministic(built_libs):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
 
 
+def test_skip_clones_keeps_the_search_identical(built_libs):
+    """Accepting children whose simulated program equals their parent's
+    without simulating them changes nothing but the number of simulations."""
+    runs = []
+    for skip in (False, True):
+        calc = OracleCalculator(SIM)
+        evo = grn.Evolution(dict(EVO, seed=13), 2, calculator=calc)
+        evo.set_skip_clones(skip)
+        st = [evo.step() for _ in range(6)]
+        models = [evo.individual(d, i) for d in range(4) for i in range(10)]
+        runs.append((st, models, sum(c[0] for c in calc.calls)))
+        evo.close()
+    (s1, m1, n1), (s2, m2, n2) = runs
+    assert all(x["n_clones"] == 0 for x in s1)
+    clones = sum(x["n_clones"] for x in s2)
+    assert clones > 0 and n2 == n1 - clones
+    assert all(a["n_evaluated"] + a["n_clones"] == 40 for a in s2)
+    assert [x["best_error"] for x in s1] == [x["best_error"] for x in s2]
+    for a, b in zip(m1, m2):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+
+
 def test_evolution_models_grow_within_limits(built_libs):
     """Duplication mutations add products; excess removal keeps the
     products and links in use within the limits."""

@@ -1,0 +1,206 @@
+"""Surrogate fitness MLP (grn_surrogate_*, grn_encode_models): the model
+encoding on the CPU, the FP64 numpy MLP's own backward pass against finite
+differences, and on the GPU the tensor-core forward/backward/Adam kernels
+against that FP64 MLP with BF16 rounding emulated at the points where the
+kernels store BF16."""
+import math
+
+import numpy as np
+import pytest
+
+import grn_b200 as grn
+import mlp_ref
+import synth
+
+N_MORPH = 2
+
+
+def _one_model_batch():
+    prods = np.zeros(2, grn.PRODUCT_DTYPE)
+    prods["label"] = [0, 1]
+    prods["lim"] = [0.5, 0.25]
+    prods["deg"] = [0.125, 0.75]
+    prods["dif"] = [0.0, 0.375]
+    links = np.zeros(3, grn.LINK_DTYPE)
+    # 1 -> 0 OR (n 1, K 1), 0 -> 1 OR (n 2, K 0.5), 1 -> 1 AND repression (n 3, K 0.25)
+    links["regulator"] = [1, 0, 1]
+    links["regulated"] = [0, 1, 1]
+    links["hill_coef"] = [1.0, 2.0, -3.0]
+    links["dis_const"] = [1.0, 0.5, 0.25]
+    links["is_and"] = [0, 0, 1]
+    return grn.ModelBatch.from_models([(prods, links)])
+
+
+def test_encoding_layout(built_libs):
+    f = grn.encode_models(_one_model_batch(), 1)[0]
+    assert f.shape == (128,)
+    np.testing.assert_allclose(f[:8], [0.5, 0.125, 0.0, 1.0, 0.25, 0.75, 0.375, 1.0], rtol=1e-7)
+    assert not f[8:32].any()  # genes 2..7 absent
+    links = f[32:44].reshape(3, 4)
+    # program order: gene 0's OR link, gene 1's OR link, gene 1's AND link
+    np.testing.assert_allclose(links[0], [1 / 8, 1.0, 1 / 5, 1 / 8], rtol=1e-6)
+    np.testing.assert_allclose(links[1], [0 / 8, 0.5, 2 / 5, 2 / 8], rtol=1e-6)
+    np.testing.assert_allclose(links[2], [1 / 8, 0.25, -3 / 5, -2 / 8], rtol=1e-6)
+    assert not f[44:].any()
+
+
+def test_encoding_batch_bounds(built_libs):
+    b = synth.random_batch(500, (2, 8), (1, 24), N_MORPH, 5)
+    f = grn.encode_models(b, N_MORPH)
+    assert f.shape == (500, 128) and np.isfinite(f).all()
+    assert np.abs(f).max() <= 4.0
+    # genes in use are flagged, and the flags are a prefix
+    flags = f[:, 3:32:4]
+    assert ((flags == 0) | (flags == 1)).all()
+    assert (np.diff(flags, axis=1) <= 0).all()
+
+
+def test_encoding_rejects_bad_model(built_libs):
+    prods = np.zeros(1, grn.PRODUCT_DTYPE)
+    links = np.zeros(1, grn.LINK_DTYPE)
+    links["regulator"], links["regulated"] = 5, 0  # regulator 5 has no product
+    links["hill_coef"], links["dis_const"] = 1.0, 0.5
+    with pytest.raises(grn.GrnError):
+        grn.encode_models(grn.ModelBatch.from_models([(prods, links)]), 1)
+
+
+def test_fp64_mlp_backward_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    P = {name: rng.normal(size=shape) * (0.1 if name[0] == "W" else 0.05)
+         for name, shape in mlp_ref.SHAPES}
+    p = mlp_ref.pack(P)
+    x = rng.normal(size=(6, 128))
+    t = rng.normal(size=6)
+    loss, g = mlp_ref.loss_and_grads(p, x, t, emulate_bf16=False)
+    offsets = np.cumsum([0] + [int(np.prod(s)) for _, s in mlp_ref.SHAPES])
+    for k, (name, _) in enumerate(mlp_ref.SHAPES):
+        n = offsets[k + 1] - offsets[k]
+        for i in rng.choice(n, min(3, n), replace=False):
+            j = offsets[k] + i
+            e = np.zeros_like(p)
+            e[j] = 1e-6
+            fd = (mlp_ref.loss_and_grads(p + e, x, t, False)[0] -
+                  mlp_ref.loss_and_grads(p - e, x, t, False)[0]) / 2e-6
+            assert abs(fd - g[j]) <= 1e-6 + 1e-5 * abs(g[j]), (name, i, fd, g[j])
+
+
+def test_surrogate_needs_device(built_libs):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(grn.GrnError) as e:
+        grn.Surrogate()
+    assert "NO_DEVICE" in str(e.value)
+
+
+def _blocks(v):
+    o, out = 0, {}
+    for name, shape in mlp_ref.SHAPES:
+        n = int(np.prod(shape))
+        out[name] = v[o:o + n]
+        o += n
+    return out
+
+
+@pytest.mark.gpu
+def test_surrogate_gradients_match_fp64(built_libs):
+    rng = np.random.default_rng(1)
+    s = grn.Surrogate(seed=11)
+    p = s.params().astype(np.float64)
+    x = rng.normal(size=(300, 128)).astype(np.float32)  # 300: ragged 64-row tiles
+    t = (rng.normal(size=300) - 1).astype(np.float32)
+    loss, g = s.gradients(x, t)
+    ref_loss, ref_g = mlp_ref.loss_and_grads(p, x, t, emulate_bf16=True)
+    _, g64 = mlp_ref.loss_and_grads(p, x, t, emulate_bf16=False)
+    assert abs(loss - ref_loss) <= 1e-4 * ref_loss
+    y = s.predict(x)
+    y_ref, _ = mlp_ref.forward(p, x, emulate_bf16=True)
+    assert np.linalg.norm(y - y_ref) <= 2e-3 * np.linalg.norm(y_ref)
+    gb, rb, fb = _blocks(g), _blocks(ref_g), _blocks(g64)
+    for name, _ in mlp_ref.SHAPES:
+        # BF16-emulating FP64 reference: the same roundings, FP64 sums (tolerance 5e-3)
+        assert np.linalg.norm(gb[name] - rb[name]) <= 5e-3 * np.linalg.norm(rb[name]), name
+        # plain FP64 gradient: BF16 operands keep the direction (cosine >= 0.99)
+        cos = gb[name] @ fb[name] / (np.linalg.norm(gb[name]) * np.linalg.norm(fb[name]))
+        assert cos >= 0.99, (name, cos)
+
+
+@pytest.mark.gpu
+def test_surrogate_adam_step(built_libs):
+    rng = np.random.default_rng(2)
+    s = grn.Surrogate(seed=12, capacity=256)
+    p0 = s.params().astype(np.float64)
+    x = rng.normal(size=(256, 128)).astype(np.float32)
+    t = rng.normal(size=256).astype(np.float32)
+    s.add_data(x, t)
+    assert s.data_count == 256
+    lr = 1e-3
+    s.train(epochs=1, batch_size=256, lr=lr)  # one minibatch: the whole set
+    p1 = s.params().astype(np.float64)
+    _, g = mlp_ref.loss_and_grads(p0, x, t, emulate_bf16=True)
+    p_ref, _, _ = mlp_ref.adam(p0, g, np.zeros_like(p0), np.zeros_like(p0), 1, lr)
+    d, d_ref = p1 - p0, p_ref - p0
+    # Adam's first step is lr * g / (|g| + eps): at most lr per parameter
+    assert np.abs(d).max() <= lr * 1.0001
+    assert np.linalg.norm(d - d_ref) <= 0.05 * np.linalg.norm(d_ref)
+
+
+@pytest.mark.gpu
+def test_surrogate_params_roundtrip_and_ring(built_libs):
+    s = grn.Surrogate(seed=13, capacity=100)
+    p = np.random.default_rng(3).normal(size=grn.N_PARAMS).astype(np.float32)
+    s.set_params(p)
+    np.testing.assert_array_equal(s.params(), p)
+    x = np.zeros((150, 128), np.float32)
+    s.add_data(x, np.zeros(150, np.float32))
+    assert s.data_count == 100  # ring buffer keeps the newest 100
+
+
+@pytest.mark.gpu
+def test_surrogate_learns_smooth_function(built_libs):
+    rng = np.random.default_rng(4)
+    n = 12000
+    X = rng.uniform(-1, 1, size=(n, 128)).astype(np.float32)
+    u = rng.normal(size=128) / math.sqrt(128)
+    v = rng.normal(size=128) / math.sqrt(128)
+    T = (np.sin(2 * X @ u) + 0.5 * (X @ v) ** 2).astype(np.float32)
+    s = grn.Surrogate(seed=14, capacity=10000)
+    s.add_data(X[:10000], T[:10000])
+    first = s.train(epochs=1, batch_size=256, lr=1e-3)
+    for _ in range(14):
+        last = s.train(epochs=1, batch_size=256, lr=1e-3)
+    assert last < 0.2 * first
+    P = s.predict(X[10000:])
+    assert np.mean((P - T[10000:]) ** 2) <= 0.15 * np.var(T[10000:])
+
+
+@pytest.mark.gpu
+def test_evolution_with_surrogate_screening(built_libs):
+    params = dict(dim_x=16, dim_y=16, n_input_morphogens=1, n_target_morphogens=1,
+                  num_sim_steps=100, error_precision=6, fitness_kind=0, dt=0.1, min_conc=0.0,
+                  min_conc_change=1e-3, dist_error_threshold=0.05)
+    wl = dict(synth.WORKLOADS["uneven_64x64"], W=16, H=16, n_exp=2)
+    init, tgt = synth.experiments(wl, 3)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        evo = grn.Evolution(dict(n_demes=4, deme_size=64, migration_period=5, n_max_products=6,
+                                 n_max_links=12, n_host_threads=2, seed=5), 2, evaluator=ev)
+        sur = grn.Surrogate(seed=6, capacity=4096)
+        evo.set_surrogate(sur, simulate_fraction=0.25, min_train_pairs=512,
+                          batches_per_generation=8, batch_size=128)
+        stats = [evo.step() for _ in range(8)]
+        # generation 0 simulates the initial 256; clones of their parent are
+        # never simulated; screening starts once 512 pairs exist
+        assert stats[0]["n_evaluated"] == 256 and stats[0]["n_screened"] == 0
+        assert all(s["n_evaluated"] + s["n_clones"] == 256 for s in stats[1:] if
+                   not s["n_screened"])
+        screened = [s for s in stats if s["n_screened"]]
+        assert screened and all(s["n_screened"] + s["n_clones"] == 256 and
+                                s["n_evaluated"] == math.ceil(0.25 * s["n_screened"])
+                                for s in screened)
+        assert sur.data_count == sum(s["n_evaluated"] for s in stats)
+        best = [s["best_error"] for s in stats]
+        assert all(b2 <= b1 for b1, b2 in zip(best, best[1:]))
+        assert all(math.isfinite(s["surrogate_loss"]) for s in stats)
+        evo.close()
+        sur.close()
