@@ -130,10 +130,12 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
   fit &= ~1;
   const int gmax = ph.max_genes;
   LaunchPlan best{};
+  best.cluster = 1;
   double best_score = -1;
   for (int i = 0; i < sim_variant_count(); ++i) {
     const KernelVariant v = sim_variant(i);
-    if (v.gmax < gmax || v.ragged != ragged || (!v.loop && Q > v.threads * v.items)) continue;
+    if (v.cluster || v.gmax < gmax || v.ragged != ragged || (!v.loop && Q > v.threads * v.items))
+      continue;
     const int planes = std::min(fit, 2 * gmax);
     const size_t smem = fixed + planes * plane_bytes;
     int occ = 0;

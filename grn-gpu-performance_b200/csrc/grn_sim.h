@@ -52,6 +52,8 @@ struct KernelVariant {
   int items;    // float4 groups each thread owns (fixed items)
   bool loop;    // threads walk the grid's groups (any grid size)
   bool ragged;  // compiled for W not a multiple of 4
+  bool cluster; // cluster-split: a cluster of CTAs per model, one band of
+                // rows each
 };
 
 // Launch plan chosen by the host.
@@ -63,12 +65,14 @@ struct LaunchPlan {
   size_t smem_bytes;     // dynamic shared memory
   int blocks_per_sm;
   int64_t slot_floats;   // floats of one block's global state slot (0: none)
+  int cluster;           // CTAs per cluster (1: one CTA per model)
 };
 
 // Floats of one state plane of a W x H grid: rows padded to float4 groups,
-// plus a zero row above and below (see the kernel's Geom).
-inline int64_t plane_floats(int W, int H) {
-  return (int64_t)(H + 2) * 4 * ((W + 3) / 4);
+// plus a zero row above and below (see the kernel's Geom).  With a cluster
+// of C CTAs per model a CTA's plane holds a band of ceil(H / C) rows.
+inline int64_t plane_floats(int W, int H, int cluster = 1) {
+  return (int64_t)((H + cluster - 1) / cluster + 2) * 4 * ((W + 3) / 4);
 }
 
 // Bytes of shared memory a block needs besides the state planes.
@@ -83,6 +87,11 @@ KernelVariant sim_variant(int i);
 // shared memory attribute as a side effect.
 cudaError_t sim_occupancy(const KernelVariant &v, size_t smem_bytes,
                           int *blocks_per_sm);
+
+// Cluster-split variant: resident clusters of `cluster` CTAs on the device
+// (0 if it does not fit).
+cudaError_t sim_cluster_occupancy(const KernelVariant &v, size_t smem_bytes, int cluster,
+                                  int *clusters);
 
 // Launches a variant; the caller has zeroed args.work_counter on `stream`.
 cudaError_t sim_launch(const LaunchPlan &plan, const SimArgs &args,

@@ -27,6 +27,7 @@
 // modelsimulatordevice.cu:44-47) and a zero rate keeps the current value
 // (the GPU kernel's double buffer keeps a two-steps-old one, :178).
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -38,7 +39,10 @@
 namespace grn {
 namespace {
 
+namespace cg = cooperative_groups;
+
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxCluster = 16;
 
 // ---- MUFU instructions (PTX ISA: lg2/ex2/rcp .approx.ftz.f32) ----------
 __device__ __forceinline__ float lg2_approx(float x) {
@@ -87,8 +91,12 @@ static_assert(sizeof(DenseSmem) % 16 == 0, "dense table is whole words");
 constexpr size_t kDenseOffset = sizeof(ModelSmem);
 constexpr size_t kRedOffset = kDenseOffset + sizeof(DenseSmem);  // float [2][32]
 constexpr size_t kDredOffset = kRedOffset + 2 * 32 * 4;  // double [32]
-constexpr size_t kWorkOffset = kDredOffset + 32 * 8;     // int
-constexpr size_t kStateOffset = (kWorkOffset + 16 + 127) & ~size_t(127);
+constexpr size_t kWorkOffset = kDredOffset + 32 * 8;     // int [2]
+// Cluster exchange slots: per-CTA step maxima float [2][kMaxCluster] (by
+// step parity) and per-CTA fitness sums double [kMaxCluster].
+constexpr size_t kCmaxOffset = kWorkOffset + 16;
+constexpr size_t kCsumOffset = kCmaxOffset + 2 * kMaxCluster * 4;
+constexpr size_t kStateOffset = (kCsumOffset + kMaxCluster * 8 + 127) & ~size_t(127);
 
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
 
@@ -281,8 +289,14 @@ __device__ __forceinline__ void build_dense(const ModelSmem &M, DenseSmem &D, in
 // reference's neighbour sum unchanged.  Steps write data groups only; when W
 // is not a multiple of 4 the cells past W of a row's last group are written
 // as 0 and serve as that row's right border.
+//
+// A cluster-split launch gives each CTA of a cluster a band of rows
+// [y0, y0 + H) of the Hg-row grid, held the same way: one halo row above and
+// one below (the neighbouring bands' edge rows, pushed into them after every
+// step, or zero at the grid border).
 struct Geom {
   int W, H, Wg, RS, PS, Q;
+  int y0, Hg;  // first grid row of the band, grid height
 };
 
 // One float4 group a thread owns, with everything a step needs about its
@@ -303,7 +317,8 @@ __device__ __forceinline__ Item make_item(int y, int gx, bool valid, int lane,
   it.valid = valid;
   it.base = (y + 1) * g.RS + 4 * gx;
   const int x0 = 4 * gx;
-  const float tv = (y > 0 ? 1.0f : 0.0f) + (y < g.H - 1 ? 1.0f : 0.0f);
+  const int yg = y + g.y0;
+  const float tv = (yg > 0 ? 1.0f : 0.0f) + (yg < g.Hg - 1 ? 1.0f : 0.0f);
   it.tot.x = tv + (x0 > 0 ? 1.0f : 0.0f) + (x0 + 1 < g.W ? 1.0f : 0.0f);
   it.tot.y = tv + 1.0f + (x0 + 2 < g.W ? 1.0f : 0.0f);
   it.tot.z = tv + 1.0f + (x0 + 3 < g.W ? 1.0f : 0.0f);
@@ -515,6 +530,41 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   }
 }
 
+// Pushes the edge rows of the new buffer (`nxt`) of every gene into the
+// neighbouring bands' halo rows: the first row to the band above (its row
+// Hb + 1), the last row to the band below (its row 0).  Shared-memory planes
+// are reached through the cluster's distributed shared memory, global slots
+// directly (a cluster's CTAs are consecutive blocks).
+template <int NT, int GMAX>
+__device__ __forceinline__ void push_halos(const SimArgs &A, const StatePtrs &sp, const Geom &g,
+                                           int G, int nxt, int rank, int C, int Hb) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int n4 = g.RS / 4;
+  for (int i = threadIdx.x; i < G * 2 * n4; i += NT) {
+    const int p = i / (2 * n4), rem = i - p * 2 * n4;
+    const int dir = rem / n4, c = rem - dir * n4;
+    const int dst = dir == 0 ? rank - 1 : rank + 1;
+    if (dst < 0 || dst >= C) continue;
+    float *pl = plane_of<GMAX>(sp, g, p, nxt);
+    const float4 v = *reinterpret_cast<const float4 *>(pl + (dir == 0 ? 1 : g.H) * g.RS + 4 * c);
+    float *dpl = p < sp.n_sm
+                     ? cl.map_shared_rank(pl, (unsigned)dst)
+                     : A.gstate + (size_t)(blockIdx.x - rank + dst) * (size_t)A.slot_floats +
+                           (pl - sp.gl);
+    *reinterpret_cast<float4 *>(dpl + (dir == 0 ? Hb + 1 : 0) * g.RS + 4 * c) = v;
+  }
+}
+
+// Cluster-wide combine of one value per CTA: CTA `rank` stores v into slot
+// `rank` of every CTA's array, then the cluster barrier (which also orders
+// the halo rows pushed before it).  Every CTA then reads the same C slots.
+template <typename T>
+__device__ __forceinline__ void cluster_share(T *slots, T v, int rank, int C) {
+  cg::cluster_group cl = cg::this_cluster();
+  if ((int)threadIdx.x < C) *cl.map_shared_rank(slots + rank, threadIdx.x) = v;
+  cl.sync();
+}
+
 // The simulation kernel.
 //   NT      threads per block
 //   GMAX    most genes (products in use) per model
@@ -523,7 +573,13 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
 //   LOOP    grids with more groups than NT * ITEMS: each thread walks its
 //           groups with incrementally updated geometry
 //   RAGGED  W is not a multiple of 4
-template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED>
+//   CL      cluster-split: a cluster of C CTAs (launch attribute) simulates
+//           one model at a time, CTA r owning rows [r*Hb, r*Hb + Hb) with
+//           Hb = ceil(H / C).  Every CTA of a cluster takes the same branches
+//           and passes the same cluster barriers: the model index, the step
+//           max and the fitness sum are shared values, identical bits in
+//           every CTA.
+template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
@@ -531,15 +587,25 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   float *s_red = reinterpret_cast<float *>(smem + kRedOffset);
   double *s_dred = reinterpret_cast<double *>(smem + kDredOffset);
   int *s_work = reinterpret_cast<int *>(smem + kWorkOffset);
+  float *s_cmax = reinterpret_cast<float *>(smem + kCmaxOffset);
+  double *s_csum = reinterpret_cast<double *>(smem + kCsumOffset);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int rank = 0, C = 1;
+  if constexpr (CL) {
+    rank = (int)cg::this_cluster().block_rank();
+    C = (int)cg::this_cluster().num_blocks();
+  }
+  const int Hb = (A.H + C - 1) / C;  // band rows (the last band may be shorter)
   Geom g;
   g.W = A.W;
-  g.H = A.H;
+  g.Hg = A.H;
+  g.y0 = rank * Hb;
+  g.H = min(A.H - g.y0, Hb);
   g.Wg = A.Wg;
   g.RS = 4 * A.Wg;
-  g.PS = (A.H + 2) * g.RS;
-  g.Q = A.H * A.Wg;
+  g.PS = (Hb + 2) * g.RS;
+  g.Q = g.H * A.Wg;
   const float dt = A.dt, min_conc = A.min_conc;
   uint4 *Mw = reinterpret_cast<uint4 *>(smem);
 
@@ -554,14 +620,31 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
     for (int i = 0; i < ITEMS; ++i) items[i] = item_at(tid + i * NT, lane, g);
   }
   // Walking items: start and per-iteration stride of (row, group column).
-  const int y0 = tid / g.Wg, gx0 = tid - y0 * g.Wg;
+  const int ty0 = tid / g.Wg, gx0 = tid - ty0 * g.Wg;
   const int dy = NT / g.Wg, dgx = NT - dy * g.Wg;
   const int n_iter = (g.Q + NT - 1) / NT;
+  // Items per thread of a full band: the same in every CTA of a cluster.
+  const int n_iter_band = (Hb * g.Wg + NT - 1) / NT;
 
-  for (;;) {
-    if (tid == 0) *s_work = atomicAdd(A.work_counter, 1);
-    __syncthreads();
-    const int m = *s_work;
+  for (int iter = 0;; ++iter) {
+    int m;
+    if constexpr (CL) {
+      // Rank 0 hands the next model to every CTA of the cluster.  Two slots
+      // by iteration parity: a CTA may still be reading this iteration's
+      // slot when rank 0 (past the next cluster barrier at the earliest)
+      // writes the following one.
+      int *slot = s_work + (iter & 1);
+      if (rank == 0 && tid == 0) {
+        const int v = atomicAdd(A.work_counter, 1);
+        for (int r = 0; r < C; ++r) *cg::this_cluster().map_shared_rank(slot, r) = v;
+      }
+      cg::this_cluster().sync();
+      m = *slot;
+    } else {
+      if (tid == 0) *s_work = atomicAdd(A.work_counter, 1);
+      __syncthreads();
+      m = *s_work;
+    }
     if (m >= A.n_models) break;
     const uint4 *rec = A.packed + A.offsets[m];
     {
@@ -582,14 +665,15 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
     const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast));
     const bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
                      M.hdr.n_links > GRN_MAX_LINKS || (sp.n_sm < G && sp.gl == nullptr) ||
-                     (!LOOP && n_iter > ITEMS);
+                     (!LOOP && n_iter_band > ITEMS);
     if (bad) {
-      if (tid == 0) {
+      if (tid == 0 && rank == 0) {
         atomicExch(A.error_flag, 1);
         A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
         if (A.steps) A.steps[orig] = 0;
       }
-      __syncthreads();
+      if constexpr (CL) cg::this_cluster().sync();
+      else __syncthreads();
       continue;
     }
 
@@ -606,18 +690,21 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       // Initial state, both buffers of every gene: input morphogen planes
       // from the experiment, the other products 0 (simstate.cpp:64-90);
       // zero rows and padding cells 0.
+      // A band's halo rows start as the neighbouring grid rows.
       const float *init = A.initial + (size_t)e * A.n_in * A.W * A.H;
       for (int i = tid; i < 2 * G * g.PS; i += NT) {
         const int kb = i / g.PS, r = i - kb * g.PS;
         const int kk = kb < G ? kb : kb - G;  // gene of this plane
-        const int y = r / g.RS - 1, x = r - (y + 1) * g.RS;
+        const int rr = r / g.RS, x = r - rr * g.RS;
+        const int y = g.y0 - 1 + rr;  // grid row
         float v = 0.0f;
-        if (kb < G && kk < A.n_in && y >= 0 && y < g.H && x < g.W)
-          v = init[((size_t)kk * g.H + y) * g.W + x];
+        if (kk < A.n_in && y >= 0 && y < g.Hg && x < g.W)
+          v = init[((size_t)kk * g.Hg + y) * g.W + x];
         float *pl = plane_of<GMAX>(sp, g, kk, kb < G ? 0 : 1);
         pl[r] = v;
       }
-      __syncthreads();
+      if constexpr (CL) cg::this_cluster().sync();
+      else __syncthreads();
 
       double change = 1.0;
       int step = 0;
@@ -632,7 +719,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
           else
             group_step<ITEMS, GMAX, false, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
         } else {
-          int y = y0, gx = gx0;
+          int y = ty0, gx = gx0;
           for (int i = 0; i < n_iter; ++i) {
             const int q = tid + i * NT;
             const bool valid = q < g.Q;
@@ -649,7 +736,14 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
             }
           }
         }
-        change = (double)block_max<NT>(mx, s_red, par, lane, warp);
+        float bm = block_max<NT>(mx, s_red, par, lane, warp);
+        if constexpr (CL) {
+          push_halos<NT, GMAX>(A, sp, g, G, par ^ 1, rank, C, Hb);
+          cluster_share(s_cmax + par * kMaxCluster, bm, rank, C);
+          bm = 0.0f;
+          for (int r = 0; r < C; ++r) bm = fmaxf(bm, s_cmax[par * kMaxCluster + r]);
+        }
+        change = (double)bm;
         par ^= 1;
         ++step;
       }
@@ -658,11 +752,12 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       if (A.state_out) {
         // Final state of this experiment, unpadded [gene][y][x].
         const int planes_out = min(G, A.state_planes);
-        float *so = A.state_out + ((size_t)orig * A.n_exp + e) * A.state_planes * g.W * g.H;
+        float *so = A.state_out + ((size_t)orig * A.n_exp + e) * A.state_planes * g.W * g.Hg;
         for (int i = tid; i < planes_out * g.W * g.H; i += NT) {
           const int kk = i / (g.W * g.H), r = i - kk * g.W * g.H;
           const int y = r / g.W, x = r - y * g.W;
-          so[i] = plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
+          so[((size_t)kk * g.Hg + g.y0 + y) * g.W + x] =
+              plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
         }
       }
 
@@ -673,7 +768,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         const int y = i / g.W, x = i - y * g.W;
         for (int kk = 0; kk < A.n_target; ++kk) {
           const double a = plane_of<GMAX>(sp, g, A.n_in + kk, par)[cell_offset(g, y, x)];
-          const double b = tgt[(size_t)kk * g.W * g.H + i];
+          const double b = tgt[((size_t)kk * g.Hg + g.y0 + y) * g.W + x];
           if (A.fitness_kind == GRN_FITNESS_MSE) {
             acc += (a - b) * (a - b);
           } else {
@@ -683,16 +778,21 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         }
       }
       double dist = block_sum<NT>(acc, s_dred, lane, warp);
+      if constexpr (CL) {
+        cluster_share(s_csum, dist, rank, C);
+        dist = 0.0;
+        for (int r = 0; r < C; ++r) dist += s_csum[r];
+      }
       if (A.fitness_kind == GRN_FITNESS_MSE)
-        dist /= (double)g.W * g.H * A.n_target;
+        dist /= (double)g.W * g.Hg * A.n_target;
       else
-        dist /= (double)(g.W * g.H);
+        dist /= (double)(g.W * g.Hg);
       // Non-convergence penalty on the running change sum
       // (evaluatormorphogens.cpp:62-65).
       if (change_sum > A.min_conc_change) dist += change_sum - A.min_conc_change;
       error += dist / A.n_exp;
     }
-    if (tid == 0) {
+    if (tid == 0 && rank == 0) {
       A.raw_error[orig] = error;
       if (A.steps) A.steps[orig] = steps_total;
     }
@@ -709,16 +809,19 @@ struct VariantEntry {
   KernelFn fn;
 };
 
-#define GRN_VARIANT(NT, GMAX, ITEMS, LOOP)                                          \
-  {{NT, GMAX, ITEMS, LOOP, false}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false>},       \
-  {{NT, GMAX, ITEMS, LOOP, true}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true>}
+#define GRN_VARIANT(NT, GMAX, ITEMS, LOOP, CL)                                         \
+  {{NT, GMAX, ITEMS, LOOP, false, CL}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL>},    \
+  {{NT, GMAX, ITEMS, LOOP, true, CL}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL>}
 
 const VariantEntry kVariants[] = {
-    GRN_VARIANT(256, 4, 1, false),  GRN_VARIANT(256, 8, 1, false),
-    GRN_VARIANT(256, 16, 1, false), GRN_VARIANT(512, 4, 2, false),
-    GRN_VARIANT(512, 8, 2, false),
-    GRN_VARIANT(512, 8, 1, true),   GRN_VARIANT(512, 16, 1, true),
-    GRN_VARIANT(256, 4, 1, true),
+    GRN_VARIANT(256, 4, 1, false, false),  GRN_VARIANT(256, 8, 1, false, false),
+    GRN_VARIANT(256, 16, 1, false, false), GRN_VARIANT(512, 4, 2, false, false),
+    GRN_VARIANT(512, 8, 2, false, false),
+    GRN_VARIANT(512, 8, 1, true, false),   GRN_VARIANT(512, 16, 1, true, false),
+    GRN_VARIANT(256, 4, 1, true, false),
+    // cluster-split
+    GRN_VARIANT(512, 8, 1, false, true),   GRN_VARIANT(512, 8, 2, false, true),
+    GRN_VARIANT(512, 8, 1, true, true),    GRN_VARIANT(512, 16, 1, true, true),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -726,7 +829,7 @@ const VariantEntry *find_variant(const KernelVariant &v) {
   for (int i = 0; i < kNumVariants; ++i) {
     const KernelVariant &k = kVariants[i].v;
     if (k.threads == v.threads && k.gmax == v.gmax && k.items == v.items &&
-        k.loop == v.loop && k.ragged == v.ragged)
+        k.loop == v.loop && k.ragged == v.ragged && k.cluster == v.cluster)
       return &kVariants[i];
   }
   return nullptr;
@@ -754,12 +857,65 @@ cudaError_t sim_occupancy(const KernelVariant &v, size_t smem_bytes, int *blocks
                                                        smem_bytes);
 }
 
+cudaError_t sim_cluster_occupancy(const KernelVariant &v, size_t smem_bytes, int cluster,
+                                  int *clusters) {
+  *clusters = 0;
+  const VariantEntry *e = find_variant(v);
+  if (!e || !v.cluster || cluster < 2 || cluster > kMaxCluster) return cudaErrorInvalidValue;
+  if (cudaFuncSetAttribute(e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(e->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster, 1, 1);
+  cfg.blockDim = dim3(v.threads, 1, 1);
+  cfg.dynamicSmemBytes = smem_bytes;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaOccupancyMaxActiveClusters(clusters, e->fn, &cfg) != cudaSuccess) {
+    *clusters = 0;
+    cudaGetLastError();
+  }
+  return cudaSuccess;
+}
+
 cudaError_t sim_launch(const LaunchPlan &plan, const SimArgs &args, cudaStream_t stream) {
   const VariantEntry *e = find_variant(plan.v);
   if (!e) return cudaErrorInvalidValue;
+  if (plan.v.cluster != (plan.cluster > 1)) return cudaErrorInvalidValue;
   cudaError_t err = cudaFuncSetAttribute(e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)plan.smem_bytes);
   if (err != cudaSuccess) return err;
+  if (plan.cluster > 1) {
+    // Whole clusters only, each band non-empty.
+    const int hb = (args.H + plan.cluster - 1) / plan.cluster;
+    if (plan.cluster > kMaxCluster || plan.blocks % plan.cluster != 0 ||
+        (plan.cluster - 1) * hb >= args.H)
+      return cudaErrorInvalidValue;
+    err = cudaFuncSetAttribute(e->fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (err != cudaSuccess) return err;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(plan.blocks, 1, 1);
+    cfg.blockDim = dim3(plan.v.threads, 1, 1);
+    cfg.dynamicSmemBytes = plan.smem_bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = plan.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, e->fn, args);
+  }
   e->fn<<<plan.blocks, plan.v.threads, plan.smem_bytes, stream>>>(args);
   return cudaGetLastError();
 }

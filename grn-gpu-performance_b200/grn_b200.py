@@ -29,7 +29,8 @@ STATUS_NAMES = {0: "GRN_OK", 1: "GRN_ERR_INVALID_ARGUMENT", 2: "GRN_ERR_NO_DEVIC
 FITNESS_REF_LOGTHRESH = 0
 FITNESS_MSE = 1
 SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1, 2, 3
-SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global"}
+SCHEDULE_CLUSTER = 4
+SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster"}
 
 
 class SimParams(ctypes.Structure):
@@ -81,7 +82,7 @@ class EvalStats(ctypes.Structure):
                 ("pack_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64), ("schedule", ctypes.c_int32),
                 ("threads_per_block", ctypes.c_int32), ("blocks", ctypes.c_int32),
-                ("reserved0", ctypes.c_int32)]
+                ("cluster_size", ctypes.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
@@ -108,6 +109,8 @@ _SIGNATURES = {
     "grn_create": ([ctypes.POINTER(_P), _I, ctypes.POINTER(SimParams)], _I),
     "grn_destroy": ([_P], _I),
     "grn_set_schedule": ([_P, _I, _I], _I),
+    "grn_set_cluster_size": ([_P, _I], _I),
+    "grn_set_autotune": ([_P, _I], _I),
     "grn_set_experiments": ([_P, _I, _P, _P], _I),
     "grn_set_experiments_rgb": ([_P, _I, _P, _P], _I),
     "grn_decode_rgb": ([_I, _I, _I, _P, _P], _I),
@@ -304,8 +307,12 @@ class Evaluator:
     def __exit__(self, *a):
         self.close()
 
-    def set_schedule(self, schedule, threads=0):
+    def set_schedule(self, schedule, threads=0, cluster_size=0):
         _check(self.lib.grn_set_schedule(self.ctx, schedule, threads), self.ctx)
+        _check(self.lib.grn_set_cluster_size(self.ctx, cluster_size), self.ctx)
+
+    def set_autotune(self, enable=True):
+        _check(self.lib.grn_set_autotune(self.ctx, int(bool(enable))), self.ctx)
 
     def set_experiments(self, initial, target):
         """initial [n_exp][n_in][H][W], target [n_exp][n_target][H][W] (float64)."""

@@ -14,7 +14,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <array>
 #include <deque>
+#include <map>
 #include <new>
 #include <string>
 #include <thread>
@@ -70,6 +72,17 @@ struct grn_ctx {
   std::vector<Job *> free_jobs;
   int forced_schedule = GRN_SCHEDULE_AUTO;
   int forced_threads = 0;
+  int forced_cluster = 0;
+  // Measured autotuning of GRN_SCHEDULE_AUTO: the fastest plan timed on a
+  // sample of the first batch of each shape, by (W, H, max genes, max links,
+  // experiments, fast path, batch-size bucket).
+  bool autotune = true;
+  struct Tuned {
+    grn::KernelVariant v;
+    int cluster, planes;
+    double ms;
+  };
+  std::map<std::array<int, 7>, Tuned> tuned;
   // minConc is 0 and the uploaded initial states are finite and
   // non-negative: the kernel's fast path then gives the same results as the
   // exact one (see the kernel's update_cell).
@@ -178,67 +191,193 @@ int host_threads() {
 // batch is scored by its resident useful threads per SM (occupancy x
 // threads that own a group), fixed items preferred over walking ones and
 // all-shared-memory state over state spilling to global slots.
-grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *out) {
+// Every feasible launch plan for a batch, with the heuristic throughput
+// score of each.
+grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models,
+                           std::vector<std::pair<double, LaunchPlan>> *out) {
   const int W = ctx->p.dim_x, H = ctx->p.dim_y;
-  const int Wg = (W + 3) / 4, Q = H * Wg;
+  const int Wg = (W + 3) / 4;
   const bool ragged = (W % 4) != 0;
-  const size_t plane_bytes = (size_t)grn::plane_floats(W, H) * sizeof(float);
   const size_t fixed = grn::sim_fixed_smem_bytes();
   const size_t optin = (size_t)ctx->smem_optin;
-  int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) : 0;
-  fit &= ~1;
   const int sched = ctx->forced_schedule;
-  double best_score = -1;
-  LaunchPlan best{};
+  static const int kClusterSizes[] = {2, 4, 8, 16};
+  out->clear();
   const int nv = grn::sim_variant_count();
   for (int i = 0; i < nv; ++i) {
     const grn::KernelVariant v = grn::sim_variant(i);
     if (v.gmax < max_genes || v.ragged != ragged) continue;
     if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
-    if (!v.loop && Q > v.threads * v.items) continue;
+    if (sched == GRN_SCHEDULE_CLUSTER && !v.cluster) continue;
+    if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_CLUSTER && v.cluster) continue;
     if (sched == GRN_SCHEDULE_FIXED_ITEMS && v.loop) continue;
     if ((sched == GRN_SCHEDULE_WALK_ITEMS || sched == GRN_SCHEDULE_GLOBAL) && !v.loop) continue;
-    const int planes = sched == GRN_SCHEDULE_GLOBAL ? 0 : std::min(fit, 2 * max_genes);
-    const bool spills = planes / 2 < max_genes;
-    const size_t smem = fixed + planes * plane_bytes;
-    int occ = 0;
-    GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &occ));
-    if (occ < 1) continue;
-    double score = (double)occ * std::min(v.threads, Q) * (v.loop ? 1.0 : 1.25) *
-                   (spills ? 0.8 : 1.0);
-    score -= 1e-3 * v.gmax;  // prefer the tighter register footprint
-    if (score > best_score) {
-      best_score = score;
-      best.v = v;
-      best.schedule = sched == GRN_SCHEDULE_GLOBAL ? GRN_SCHEDULE_GLOBAL
-                      : v.loop                     ? GRN_SCHEDULE_WALK_ITEMS
-                                                   : GRN_SCHEDULE_FIXED_ITEMS;
-      best.planes = planes;
-      best.smem_bytes = smem;
-      best.blocks_per_sm = occ;
-      best.slot_floats = spills ? 2LL * v.gmax * grn::plane_floats(W, H) : 0;
+    for (int ci = 0; ci < (v.cluster ? 4 : 1); ++ci) {
+      const int C = v.cluster ? kClusterSizes[ci] : 1;
+      if (v.cluster && ctx->forced_cluster && C != ctx->forced_cluster) continue;
+      const int Hb = (H + C - 1) / C;
+      if (C > 1 && (C - 1) * Hb >= H) continue;  // every band non-empty
+      const int Qb = Hb * Wg;
+      if (!v.loop && Qb > v.threads * v.items) continue;
+      const size_t plane_bytes = (size_t)grn::plane_floats(W, H, C) * sizeof(float);
+      int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) : 0;
+      fit &= ~1;
+      // Under AUTO a walking variant whose genes spill is also offered with
+      // every plane in global memory (the L1 then caches more of them).
+      const int smem_planes = std::min(fit, 2 * max_genes);
+      const bool offer_global = sched == GRN_SCHEDULE_AUTO && v.loop && C == 1 &&
+                                smem_planes / 2 < max_genes && smem_planes > 0;
+      for (int gv = 0; gv < (offer_global ? 2 : 1); ++gv) {
+        const int planes = (sched == GRN_SCHEDULE_GLOBAL || gv == 1) ? 0 : smem_planes;
+        const bool spills = planes / 2 < max_genes;
+        const size_t smem = fixed + planes * plane_bytes;
+        int ctas = 0, per_sm = 0;  // resident CTAs on the device
+        if (C == 1) {
+          GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &per_sm));
+          ctas = per_sm * ctx->n_sm;
+        } else {
+          int clusters = 0;
+          GRN_CUDA(ctx, grn::sim_cluster_occupancy(v, smem, C, &clusters));
+          ctas = clusters * C;
+          per_sm = 1;
+        }
+        if (ctas < 1) continue;
+        // Throughput model: busy threads (no more CTAs than models need),
+        // fixed items ahead of walking ones, and a penalty for genes kept in
+        // global memory -- mild while every resident CTA's slot fits in L2.
+        const double busy = (double)std::min(ctas, n_models * C) * std::min(v.threads, Qb);
+        const double spill_frac = spills ? 1.0 - (double)(planes / 2) / max_genes : 0.0;
+        const double slot_bytes = spills ? 2.0 * v.gmax * plane_bytes : 0.0;
+        const bool l2 = slot_bytes * ctas <= 80e6;
+        double score = busy * (v.loop ? 1.0 : 1.25) * (1.0 - (l2 ? 0.3 : 0.7) * spill_frac);
+        // One cluster barrier per step costs about as much as a step of a
+        // small band (measured): clusters only as a last resort unmeasured.
+        if (C > 1) score *= 0.3 - 0.01 * C;
+        if (gv == 1) score *= 0.9;
+        score -= 1e-3 * v.gmax;  // prefer the tighter register footprint
+        LaunchPlan plan{};
+        plan.v = v;
+        plan.schedule = C > 1                                      ? GRN_SCHEDULE_CLUSTER
+                        : (sched == GRN_SCHEDULE_GLOBAL || gv == 1) ? GRN_SCHEDULE_GLOBAL
+                        : v.loop                                    ? GRN_SCHEDULE_WALK_ITEMS
+                                                                    : GRN_SCHEDULE_FIXED_ITEMS;
+        plan.planes = planes;
+        plan.smem_bytes = smem;
+        plan.blocks_per_sm = per_sm;
+        plan.slot_floats = spills ? 2LL * v.gmax * grn::plane_floats(W, H, C) : 0;
+        plan.cluster = C;
+        plan.blocks = C > 1 ? C * std::max(1, std::min(n_models, ctas / C))
+                            : std::max(1, std::min(n_models, ctas));
+        out->push_back({score, plan});
+      }
     }
   }
-  if (best_score < 0)
+  if (out->empty())
     return fail(ctx, GRN_ERR_CAPACITY, "no kernel variant holds " + std::to_string(max_genes) +
                                            " genes on this grid with this schedule");
-  best.blocks = std::max(1, std::min(n_models, ctx->n_sm * best.blocks_per_sm));
-  *out = best;
+  std::stable_sort(out->begin(), out->end(),
+                   [](const std::pair<double, LaunchPlan> &a,
+                      const std::pair<double, LaunchPlan> &b) { return a.first > b.first; });
+  return GRN_OK;
+}
+
+grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *out) {
+  std::vector<std::pair<double, LaunchPlan>> plans;
+  grn_status s = enumerate_plans(ctx, max_genes, n_models, &plans);
+  if (s != GRN_OK) return s;
+  *out = plans[0].second;
+  return GRN_OK;
+}
+
+bool same_plan(const LaunchPlan &a, const grn::KernelVariant &v, int cluster, int planes) {
+  return a.v.threads == v.threads && a.v.gmax == v.gmax && a.v.items == v.items &&
+         a.v.loop == v.loop && a.v.ragged == v.ragged && a.v.cluster == v.cluster &&
+         a.cluster == cluster && a.planes == planes;
+}
+
+// Launches the simulation of `n_models` packed records already on the
+// device.  `stream` may differ from the context's stream.
+grn_status launch_plan(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs a, cudaStream_t stream) {
+  a.planes = plan.planes;
+  a.gstate = nullptr;
+  a.slot_floats = 0;
+  if (plan.slot_floats > 0) {
+    grn_status s =
+        ensure_dev(ctx, &ctx->d_gstate, (size_t)plan.slot_floats * plan.blocks * sizeof(float));
+    if (s != GRN_OK) return s;
+    a.gstate = static_cast<float *>(ctx->d_gstate.p);
+    a.slot_floats = plan.slot_floats;
+  }
+  GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int32_t), stream));
+  GRN_CUDA(ctx, grn::sim_launch(plan, a, stream));
+  return GRN_OK;
+}
+
+// Measured autotuning: times the feasible plans (best heuristic scores
+// first, at most 8) on the batch's first models -- the most expensive ones,
+// the host orders records by cost -- with the step count capped, one
+// untimed and one timed launch each, and keeps the fastest.  The sample
+// launches write outputs of the sampled models that the real launch then
+// overwrites.  Synchronises `stream` once per new batch shape.
+grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, LaunchPlan>> &plans,
+                         const grn::SimArgs &a, int n_models, cudaStream_t stream,
+                         LaunchPlan *out) {
+  grn::SimArgs t = a;
+  t.n_models = std::min(n_models, 2 * ctx->n_sm);
+  t.n_steps = std::min(a.n_steps, 64);
+  t.state_out = nullptr;
+  t.state_planes = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  GRN_CUDA(ctx, cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(ctx, GRN_ERR_CUDA, "cudaEventCreate");
+  }
+  double best_ms = 1e30;
+  int best = -1;
+  grn_status s = GRN_OK;
+  const int n_try = std::min<int>((int)plans.size(), 8);
+  for (int i = 0; i < n_try && s == GRN_OK; ++i) {
+    const LaunchPlan p = plans[i].second;
+    const int ctas = p.blocks;  // resident CTAs for the full batch (>= sample's)
+    LaunchPlan ps = p;
+    ps.blocks = std::max(std::max(1, p.cluster),
+                         std::min(ctas, std::max(1, p.cluster) * t.n_models));
+    ps.blocks -= ps.blocks % std::max(1, p.cluster);
+    s = launch_plan(ctx, ps, t, stream);
+    if (s != GRN_OK) break;
+    if (cudaEventRecord(e0, stream) != cudaSuccess) s = fail(ctx, GRN_ERR_CUDA, "event");
+    if (s == GRN_OK) s = launch_plan(ctx, ps, t, stream);
+    if (s == GRN_OK && (cudaEventRecord(e1, stream) != cudaSuccess ||
+                        cudaEventSynchronize(e1) != cudaSuccess))
+      s = fail(ctx, GRN_ERR_CUDA, "autotune timing");
+    float ms = 0;
+    if (s == GRN_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s != GRN_OK) return s;
+  if (best < 0) return fail(ctx, GRN_ERR_CUDA, "autotune timed no plan");
+  *out = plans[best].second;
   return GRN_OK;
 }
 
 // Launches the simulation of `n_models` packed records already on the
 // device.  `stream` may differ from the context's stream.
 grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
-                         int n_models, int max_genes, const double *d_max_error,
-                         double *d_raw, int32_t *d_steps, int32_t *d_flag,
-                         cudaStream_t stream, LaunchPlan *plan_out,
+                         int n_models, int max_genes, int max_links,
+                         const double *d_max_error, double *d_raw, int32_t *d_steps,
+                         int32_t *d_flag, cudaStream_t stream, LaunchPlan *plan_out,
                          float *d_states = nullptr, int state_planes = 0) {
   if (n_models == 0) return GRN_OK;
   if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
-  LaunchPlan plan;
-  grn_status s = choose_plan(ctx, max_genes, n_models, &plan);
+  std::vector<std::pair<double, LaunchPlan>> plans;
+  grn_status s = enumerate_plans(ctx, max_genes, n_models, &plans);
   if (s != GRN_OK) return s;
+  LaunchPlan plan = plans[0].second;
   const int W = ctx->p.dim_x, H = ctx->p.dim_y, Wg = (W + 3) / 4;
   grn::SimArgs a{};
   a.packed = d_words;
@@ -267,14 +406,28 @@ grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_of
   a.state_out = d_states;
   a.state_planes = state_planes;
   a.fast_ok = ctx->fast_ok ? 1 : 0;
-  if (plan.slot_floats > 0) {
-    s = ensure_dev(ctx, &ctx->d_gstate, (size_t)plan.slot_floats * plan.blocks * sizeof(float));
-    if (s != GRN_OK) return s;
-    a.gstate = static_cast<float *>(ctx->d_gstate.p);
-    a.slot_floats = plan.slot_floats;
+  if (ctx->forced_schedule == GRN_SCHEDULE_AUTO && ctx->autotune && plans.size() > 1) {
+    const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
+    const std::array<int, 7> key = {W, H, max_genes, max_links, ctx->n_exp,
+                                    ctx->fast_ok ? 1 : 0, bucket};
+    auto it = ctx->tuned.find(key);
+    bool found = false;
+    if (it != ctx->tuned.end()) {
+      for (const auto &c : plans)
+        if (same_plan(c.second, it->second.v, it->second.cluster, it->second.planes)) {
+          plan = c.second;
+          found = true;
+          break;
+        }
+    }
+    if (!found) {
+      s = autotune_plan(ctx, plans, a, n_models, stream, &plan);
+      if (s != GRN_OK) return s;
+      ctx->tuned[key] = grn_ctx::Tuned{plan.v, plan.cluster, plan.planes, 0.0};
+    }
   }
-  GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int32_t), stream));
-  GRN_CUDA(ctx, grn::sim_launch(plan, a, stream));
+  s = launch_plan(ctx, plan, a, stream);
+  if (s != GRN_OK) return s;
   if (plan_out) *plan_out = plan;
   return GRN_OK;
 }
@@ -322,7 +475,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   GRN_CUDA(ctx, cudaEventRecord(j->ev_start, st));
   LaunchPlan plan{};
   s = launch_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
-                    static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes,
+                    static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes, ph.max_links,
                     static_cast<const double *>(j->d_maxerr.p),
                     static_cast<double *>(j->d_raw.p), static_cast<int32_t *>(j->d_steps.p),
                     static_cast<int32_t *>(j->d_flag.p), st, &plan);
@@ -342,6 +495,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
     stats->schedule = plan.schedule;
     stats->threads_per_block = plan.v.threads;
     stats->blocks = plan.blocks;
+    stats->cluster_size = std::max(1, plan.cluster);
   }
   return GRN_OK;
 }
@@ -456,9 +610,25 @@ grn_status grn_destroy(grn_ctx *ctx) {
   return GRN_OK;
 }
 
+grn_status grn_set_autotune(grn_ctx *ctx, int enable) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  ctx->autotune = enable != 0;
+  ctx->tuned.clear();
+  return GRN_OK;
+}
+
+grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (cluster_size != 0 && cluster_size != 2 && cluster_size != 4 && cluster_size != 8 &&
+      cluster_size != 16)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "cluster size must be 0, 2, 4, 8 or 16");
+  ctx->forced_cluster = cluster_size;
+  return GRN_OK;
+}
+
 grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block) {
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
-  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_GLOBAL || threads_per_block < 0)
+  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_CLUSTER || threads_per_block < 0)
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad schedule");
   ctx->forced_schedule = schedule;
   ctx->forced_threads = threads_per_block;
@@ -578,7 +748,7 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
   chk(cudaMemsetAsync(d_states.p, 0, sb, st));
   if (e == cudaSuccess) {
     s = launch_packed(ctx, static_cast<const uint4 *>(j.d_words.p),
-                      static_cast<const int32_t *>(j.d_offsets.p), n, ph.max_genes,
+                      static_cast<const int32_t *>(j.d_offsets.p), n, ph.max_genes, ph.max_links,
                       static_cast<const double *>(j.d_maxerr.p), static_cast<double *>(j.d_raw.p),
                       static_cast<int32_t *>(j.d_steps.p), static_cast<int32_t *>(j.d_flag.p), st,
                       nullptr, static_cast<float *>(d_states.p), max_planes);
@@ -738,7 +908,7 @@ grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_ma
   GRN_CUDA(ctx, cudaMemsetAsync(ctx->sync_job.d_flag.p, 0, 4, st));
   return launch_packed(ctx, static_cast<const uint4 *>(pk->d_words.p),
                        static_cast<const int32_t *>(pk->d_offsets.p), pk->host.n_models,
-                       pk->host.max_genes, d_max_error, d_raw_error, d_steps,
+                       pk->host.max_genes, pk->host.max_links, d_max_error, d_raw_error, d_steps,
                        static_cast<int32_t *>(ctx->sync_job.d_flag.p), st, nullptr);
 }
 

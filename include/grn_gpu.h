@@ -147,7 +147,7 @@ typedef struct grn_eval_stats {
   int32_t schedule;          /* grn_schedule chosen for the launch        */
   int32_t threads_per_block;
   int32_t blocks;
-  int32_t reserved0;
+  int32_t cluster_size;      /* CTAs per model (GRN_SCHEDULE_CLUSTER), else 1 */
 } grn_eval_stats;
 
 /* Kernel schedules.  GRN_SCHEDULE_AUTO lets the autotuner pick.  Every
@@ -159,8 +159,12 @@ typedef enum grn_schedule {
                                    4 cells for the whole launch           */
   GRN_SCHEDULE_WALK_ITEMS = 2,  /* threads walk the grid's groups; any
                                    grid size                              */
-  GRN_SCHEDULE_GLOBAL = 3       /* walking groups, every plane in global
+  GRN_SCHEDULE_GLOBAL = 3,      /* walking groups, every plane in global
                                    memory                                 */
+  GRN_SCHEDULE_CLUSTER = 4      /* cluster-split: a thread-block cluster
+                                   per model, each CTA a band of rows in
+                                   its shared memory, halo rows exchanged
+                                   through distributed shared memory      */
 } grn_schedule;
 
 typedef struct grn_ctx grn_ctx;
@@ -190,6 +194,19 @@ int grn_abi_version(void);
  * restore).  Returns GRN_ERR_CAPACITY later, at launch, if the forced
  * schedule cannot hold the batch. */
 grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block);
+
+/* CTAs per cluster for GRN_SCHEDULE_CLUSTER (2, 4, 8 or 16; 0: the
+ * autotuner's choice). */
+grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size);
+
+/* GRN_SCHEDULE_AUTO's plan choice.  enable = 1 (default): measured -- on the
+ * first batch of each shape (W, H, most genes, most links, experiments,
+ * fast path, batch size below 2 x SMs) up to 8 feasible plans are timed on
+ * the batch's most expensive models with at most 64 steps, and the fastest
+ * is kept for later batches of that shape (that first call synchronises its
+ * stream).  enable = 0: an occupancy/spill heuristic, no timing.  Either
+ * call clears the cache. */
+grn_status grn_set_autotune(grn_ctx *ctx, int enable);
 
 /* ------------------------------------------------------------ experiments */
 

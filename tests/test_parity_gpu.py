@@ -186,6 +186,75 @@ def test_schedules_agree_bitwise():
     assert_raw_close(base_raw, oraw, what="schedules")
 
 
+@pytest.mark.parametrize("W,H,clusters", [(36, 20, (2, 4)), (30, 37, (2, 4, 8)),
+                                           (64, 64, (2, 4, 16)), (100, 100, (4, 8))])
+def test_cluster_schedule_matches_one_cta_bitwise(W, H, clusters):
+    """A cluster of CTAs per model, each with a band of rows and halo rows
+    pushed through distributed shared memory, runs the same per-cell
+    arithmetic as one CTA per model: identical states."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=15, n_models=24, steps=60,
+                                              W=W, H=H, n_exp=2)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_WALK_ITEMS)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=8)
+        for c in clusters:
+            ev.set_schedule(grn.SCHEDULE_CLUSTER, cluster_size=c)
+            raw, states = ev.evaluate_states(batch, max_planes=8)
+            _, raw_b, st = ev.evaluate_batch(batch)
+            assert st["schedule"] == grn.SCHEDULE_CLUSTER and st["cluster_size"] == c
+            assert np.array_equal(raw, raw_b)
+            assert np.array_equal(states, base_states), c
+            assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="cluster %d" % c)
+    oe, oraw, _ = oracle.evaluate_batch(params, init, tgt, batch)
+    assert_raw_close(base_raw, oraw, what="cluster base")
+
+
+def test_cluster_schedule_with_global_genes():
+    """256 x 256 with 8 genes: a 16-CTA cluster keeps 6 genes' bands in
+    shared memory and 2 in global slots; halo rows of both kinds."""
+    params, batch, init, tgt = synth.workload("large_256x256", seed=16, n_models=6, steps=40)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=8)
+        for c in (8, 16):
+            ev.set_schedule(grn.SCHEDULE_CLUSTER, cluster_size=c)
+            raw, states = ev.evaluate_states(batch, max_planes=8)
+            assert np.array_equal(states, base_states), c
+            assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="cluster %d" % c)
+
+
+def test_autotuned_plan_is_cached_and_exact():
+    """The measured autotuner picks one plan per batch shape and keeps it;
+    whatever it picks computes the same states as the heuristic's plan."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=18, n_models=300, steps=50)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_autotune(False)
+        h_raw, h_states = ev.evaluate_states(batch, max_planes=8)
+        ev.set_autotune(True)
+        _, raw1, st1 = ev.evaluate_batch(batch)
+        _, raw2, st2 = ev.evaluate_batch(batch)
+        a_raw, a_states = ev.evaluate_states(batch, max_planes=8)
+    keys = ("schedule", "threads_per_block", "cluster_size", "blocks")
+    assert [st1[k] for k in keys] == [st2[k] for k in keys]
+    assert np.array_equal(raw1, raw2) and np.array_equal(raw1, a_raw)
+    assert np.array_equal(a_states, h_states)
+    assert_raw_close(a_raw, h_raw, rtol=1e-12, atol=0, what="autotune")
+
+
+def test_cluster_schedule_rejects_empty_bands():
+    params, batch, init, tgt = synth.workload("small_32x32", seed=17, n_models=4, steps=10,
+                                              W=32, H=20)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_CLUSTER, cluster_size=16)  # 15 * 2 rows >= 20
+        with pytest.raises(grn.GrnError) as e:
+            ev.evaluate_batch(batch)
+        assert "CAPACITY" in str(e.value)
+
+
 def test_early_exit_and_steps():
     """minConcChange stops simulations early; the non-convergence penalty
     uses the running change sum."""
