@@ -15,9 +15,14 @@ uneven_64x64: 4096 models, 2-8 genes, 1-24 links, 64x64 grid, 2000 steps).
           host compile of the batch, pinned H2D copy, kernel, D2H of the raw
           errors and host rounding inside the timed region (wall clock,
           synchronised on both sides).
-  roofline  MUFU (SFU pipe) bound: algorithmic MUFU ops of a launch (lg2 per
-          regulator gene, ex2 + rcp per regulated gene, per cell-step) over
-          the mean launch time, against 16 MUFU/clk/SM x SMs x max SM clock.
+  roofline  MUFU (SFU pipe) bound.  achieved = algorithmic MUFU ops of a
+          launch -- 3 per used link per cell-update (lg2, ex2, rcp of each
+          Hill term in the reference formulation) -- over the mean launch
+          time, against 16 MUFU/clk/SM x SMs x max SM clock.  The kernel
+          issues fewer MUFU ops than that (one lg2 per regulator product and
+          one ex2 + rcp per regulated product, in exponent form); those are
+          reported as issued_mufu.  fp32_frac: algorithmic FP32 ops
+          (6 L + 7 G + 8 G_dif per cell-update) against 128/clk/SM.
   cpu_baseline  the FP64 oracle (a port of the reference's CPU evaluator) on
           the host cores, on a bounded sample of the same workload.
 
@@ -44,6 +49,7 @@ sys.path.insert(0, os.path.join(ROOT, "grn-gpu-performance_b200"))
 import synth  # noqa: E402
 
 SFU_PER_CLK_PER_SM = 16  # MUFU results per clock per SM (lg2/ex2/rcp, FP32)
+FP32_PER_CLK_PER_SM = 128  # FP32 lanes per SM
 
 
 def read_peaks():
@@ -341,9 +347,12 @@ def main():
     # sfu_ops_per_step sums every model's MUFU ops of one Euler step over the
     # grid; steps_run / n is the Euler steps each model ran (all equal here:
     # min_conc_change 0 never stops a simulation early).
-    sfu_ops = info["sfu_ops_per_step"] * (steps_run / max(n, 1))
-    achieved = sfu_ops / (mean_ms / 1000.0) / 1e9
+    model_steps = steps_run / max(n, 1)
+    achieved = info["alg_sfu_ops_per_step"] * model_steps / (mean_ms / 1000.0) / 1e9
+    issued = info["sfu_ops_per_step"] * model_steps / (mean_ms / 1000.0) / 1e9
+    fp32 = info["alg_fp32_ops_per_step"] * model_steps / (mean_ms / 1000.0) / 1e9
     peak = SFU_PER_CLK_PER_SM * n_sm * sm_max * 1e6 / 1e9
+    fp32_peak = FP32_PER_CLK_PER_SM * n_sm * sm_max * 1e6 / 1e9
     prof = read_profile(args.workload)
     value = n * world * args.steps / (total_ms / 1000.0)
     line = {
@@ -387,6 +396,10 @@ def main():
             "peak": peak,
             "unit": "Gop/s (MUFU lg2/ex2/rcp)",
             "frac": achieved / peak,
+            "algorithmic": "3 MUFU ops per used link per cell-update (mean %.3f links)" % (
+                info["mean_links"]),
+            "issued_mufu": {"achieved": issued, "frac": issued / peak},
+            "fp32_frac": fp32 / fp32_peak,
             "peak_source": "16 MUFU/clk/SM x %d SMs x %.0f MHz (%s sm_max_mhz)" % (
                 n_sm, sm_max, peak_kind),
             "traffic": prof.get("dram_bytes_per_launch") if prof else None,

@@ -92,7 +92,10 @@ class PackedInfo(ctypes.Structure):
     _fields_ = [("n_models", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("cell_update_bound", ctypes.c_int64), ("sfu_ops_per_step", ctypes.c_int64),
                 ("max_genes", ctypes.c_int32), ("max_links", ctypes.c_int32),
-                ("mean_genes", ctypes.c_double), ("mean_links", ctypes.c_double)]
+                ("mean_genes", ctypes.c_double), ("mean_links", ctypes.c_double),
+                ("mean_dif_genes", ctypes.c_double),
+                ("alg_sfu_ops_per_step", ctypes.c_int64),
+                ("alg_fp32_ops_per_step", ctypes.c_int64)]
 
 
 _P = ctypes.c_void_p

@@ -893,6 +893,9 @@ grn_status grn_packed_get_info(const grn_packed *pk, grn_packed_info *info) {
   info->max_links = h.max_links;
   info->mean_genes = h.n_models ? h.sum_genes / h.n_models : 0;
   info->mean_links = h.n_models ? h.sum_links / h.n_models : 0;
+  info->mean_dif_genes = h.n_models ? h.sum_dif_genes / h.n_models : 0;
+  info->alg_sfu_ops_per_step = h.alg_sfu_per_cell_step * cells;
+  info->alg_fp32_ops_per_step = h.alg_fp32_per_cell_step * cells;
   return GRN_OK;
 }
 

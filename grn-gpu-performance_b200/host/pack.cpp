@@ -214,6 +214,8 @@ grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
   out->max_genes = out->max_links = 0;
   out->sum_genes = out->sum_links = 0;
   out->sfu_per_cell_step = out->fma_per_cell_step = 0;
+  out->sum_dif_genes = 0;
+  out->alg_sfu_per_cell_step = out->alg_fp32_per_cell_step = 0;
   for (int i = 0; i < n; ++i) {
     const int m = order[i];
     out->offsets[i] = (int32_t)out->words.size();
@@ -225,6 +227,9 @@ grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
     out->sum_links += c.links;
     out->sfu_per_cell_step += c.lg_genes + 2 * c.reg_genes;
     out->fma_per_cell_step += 2 * c.links + 6 * c.genes + 6 * c.dif_genes;
+    out->sum_dif_genes += c.dif_genes;
+    out->alg_sfu_per_cell_step += 3 * c.links;
+    out->alg_fp32_per_cell_step += 6 * c.links + 7 * c.genes + 8 * c.dif_genes;
   }
   return GRN_OK;
 }

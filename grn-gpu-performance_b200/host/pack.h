@@ -43,6 +43,9 @@ struct PackedHost {
   double sum_links = 0;
   int64_t sfu_per_cell_step = 0;  // sum over models of lg + 2 * reg genes
   int64_t fma_per_cell_step = 0;  // rough FP32-pipe op count, summed
+  double sum_dif_genes = 0;
+  int64_t alg_sfu_per_cell_step = 0;   // sum of 3 L (reference formulation)
+  int64_t alg_fp32_per_cell_step = 0;  // sum of 6 L + 7 G + 8 G_dif
 };
 
 grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,

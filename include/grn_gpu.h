@@ -298,6 +298,13 @@ typedef struct grn_packed_info {
   int32_t max_links;         /* largest used-link count                   */
   double mean_genes;
   double mean_links;
+  double mean_dif_genes;     /* diffusing products in use per model       */
+  /* Algorithmic work of one Euler step of all models, counted on the
+   * reference formulation: 3 MUFU ops (lg2, ex2, rcp) per used link and
+   * cell, and 6 L + 7 G + 8 G_dif FP32 ops per cell (L used links, G
+   * products in use, G_dif of them diffusing). */
+  int64_t alg_sfu_ops_per_step;
+  int64_t alg_fp32_ops_per_step;
 } grn_packed_info;
 grn_status grn_packed_get_info(const grn_packed *packed, grn_packed_info *info);
 
