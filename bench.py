@@ -198,15 +198,24 @@ def run_evolution(args, rank, world):
     ev = grn.Evaluator(params, device=torch.cuda.current_device())
     ev.set_experiments(init, tgt)
     evo = grn.Evolution(evo_p, wl["n_in"] + wl["n_target"], evaluator=ev)
+    if args.skip_clones:
+        evo.set_skip_clones(True)
+    isl = None
+    if world > 1:
+        import sharded
+        isl = sharded.IslandShards(evo, n_demes, deme, period=10, seed=args.seed)
     gens = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        st = evo.step()
+        st = isl.step() if isl else evo.step()
         st["wall_ms"] = 1000 * (time.perf_counter() - t0)
         gens.append(st)
     timed = gens[args.warmup:]
     wall = sum(g["wall_ms"] for g in timed) / 1000.0
-    n_eval = sum(g["n_evaluated"] for g in timed)
+    # Children whose fitness was settled: simulated, or accepted as clones of
+    # their parent (--skip-clones; exact, see grn_evolution_set_skip_clones).
+    n_sim = sum(g["n_evaluated"] for g in timed)
+    n_eval = n_sim + sum(g["n_clones"] for g in timed)
     if rank == 0:
         line = {
             "metric": "GRN fitness evals/sec", "value": n_eval * world / wall, "unit": "evals/s",
@@ -216,10 +225,14 @@ def run_evolution(args, rank, world):
             "config": {"workload": args.workload, "demes": n_demes, "deme_size": deme,
                        "grid": "%dx%d" % (wl["W"], wl["H"]), "euler_steps": wl["steps"],
                        "step": "one generation (reproduce, evaluate, select)",
+                       "skip_clones": bool(args.skip_clones),
+                       "migration": "demes every 10 generations; across ranks every 10"
+                                    if world > 1 else "demes every 10 generations",
                        "l2": "state and inputs exceed no cache; timed by wall clock per generation"},
             "generations": [{k: round(v, 6) if isinstance(v, float) else v
                              for k, v in g.items()} for g in gens],
             "eval_fraction": sum(g["eval_ms"] for g in timed) / (1000 * wall),
+            "simulated_per_s": n_sim * world / wall,
         }
         print(json.dumps(line), flush=True)
     evo.close()
@@ -237,6 +250,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--skip-clones", action="store_true",
+                    help="island workloads: accept children whose simulated program equals "
+                         "their parent's without simulating them")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -137,6 +137,8 @@ _SIGNATURES = {
     "grn_evolution_best": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "grn_evolution_destroy": ([_P], _I),
     "grn_encode_models": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
+    "grn_model_costs": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
+    "grn_evolution_set_individual": ([_P, _I, _I, _P, _I, _P, _I, _D], _I),
     "grn_surrogate_create": ([_I, ctypes.c_uint64, _I, ctypes.POINTER(_P)], _I),
     "grn_surrogate_destroy": ([_P], _I),
     "grn_surrogate_add_data": ([_P, _P, _P, _I], _I),
@@ -484,6 +486,13 @@ class Evolution:
                                                  None, None))
         return prods, links, err.value, c.value
 
+    def set_individual(self, deme, index, products, links, error):
+        p = np.ascontiguousarray(products, PRODUCT_DTYPE)
+        l = np.ascontiguousarray(links, LINK_DTYPE)
+        _check(self.lib.grn_evolution_set_individual(
+            self.handle, deme, index, _ptr(p) if len(p) else None, len(p),
+            _ptr(l) if len(l) else None, len(l), float(error)))
+
     def set_skip_clones(self, enable=True):
         _check(self.lib.grn_evolution_set_skip_clones(self.handle, int(bool(enable))))
 
@@ -513,6 +522,14 @@ class Evolution:
 
 N_FEATURES = 128
 N_PARAMS = 164865
+
+
+def model_costs(batch, n_morphogens):
+    """grn_model_costs: relative work of one cell-step of each model."""
+    out = np.zeros(batch.n_models, np.float64)
+    cb = batch.as_c()
+    _check(load_library().grn_model_costs(ctypes.byref(cb), n_morphogens, _ptr(out)))
+    return out
 
 
 def encode_models(batch, n_morphogens):

@@ -917,6 +917,26 @@ grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_ma
 
 }  // extern "C"
 
+extern "C" grn_status grn_model_costs(const grn_model_batch *batch, int n_morphogens,
+                                      double *cost_out) {
+  if (!batch || !cost_out || batch->n_models < 0 || n_morphogens < 0 ||
+      (batch->n_models > 0 && (!batch->product_offsets || !batch->link_offsets)))
+    return GRN_ERR_INVALID_ARGUMENT;
+  for (int m = 0; m < batch->n_models; ++m) {
+    const int p0 = batch->product_offsets[m], p1 = batch->product_offsets[m + 1];
+    const int l0 = batch->link_offsets[m], l1 = batch->link_offsets[m + 1];
+    if (p1 < p0 || l1 < l0) return GRN_ERR_INVALID_ARGUMENT;
+    std::vector<uint4> rec;
+    grn::ModelCost cost;
+    std::string err;
+    const grn_status s = grn::pack_model(batch->products + p0, p1 - p0, batch->links + l0,
+                                         l1 - l0, n_morphogens, m, &rec, &cost, &err);
+    if (s != GRN_OK) return s;
+    cost_out[m] = cost.cost;
+  }
+  return GRN_OK;
+}
+
 extern "C" grn_status grn_describe_model(const grn_product *products, int n_products,
                                          const grn_link *links, int n_links, int n_morphogens,
                                          char *buf, int buf_len) {

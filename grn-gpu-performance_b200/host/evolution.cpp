@@ -768,6 +768,21 @@ grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int inde
   return GRN_OK;
 }
 
+grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
+                                        const grn_product *products, int n_products,
+                                        const grn_link *links, int n_links, double error) {
+  if (!evo || deme < 0 || deme >= (int)evo->demes.size() || index < 0 ||
+      index >= (int)evo->demes[deme].pop.size() || n_products < 0 || n_links < 0 ||
+      (n_products && !products) || (n_links && !links))
+    return GRN_ERR_INVALID_ARGUMENT;
+  Individual &ind = evo->demes[deme].pop[index];
+  ind.model.prods.assign(products, products + n_products);
+  ind.model.links.assign(links, links + n_links);
+  ind.error = error;
+  ind.complexity = evo->ops.complexity_in_use(ind.model);
+  return GRN_OK;
+}
+
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index) {
   if (!evo || !deme || !index || evo->generation < 0) return GRN_ERR_INVALID_ARGUMENT;
   double best = 1e300;

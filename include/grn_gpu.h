@@ -330,6 +330,11 @@ grn_status grn_describe_model(const grn_product *products, int n_products,
                               const grn_link *links, int n_links,
                               int n_morphogens, char *buf, int buf_len);
 
+/* Relative simulation work of one cell-step of each model of a batch (host
+ * only; the weights the evaluator uses to order its work queue), for
+ * splitting a batch into equal-work shards across GPUs. */
+grn_status grn_model_costs(const grn_model_batch *batch, int n_morphogens, double *cost_out);
+
 /* ------------------------------------------------- island evolution ---
  * Deterministic-crowding island search over GRN models, the reference's
  * Search + SearchAlgoDetCrowd (Src/Search/search.cpp:101-311,
@@ -393,6 +398,11 @@ grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int inde
                                     int *n_products, grn_link *links, int max_links,
                                     int *n_links, double *error, int *complexity);
 /* Position of the best individual (lowest error, then lowest complexity). */
+/* Replaces individual `index` of deme `deme` (migration between searches,
+ * e.g. islands on other GPUs): the model and its known error. */
+grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
+                                        const grn_product *products, int n_products,
+                                        const grn_link *links, int n_links, double error);
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index);
 grn_status grn_evolution_destroy(grn_evolution *evo);
 

@@ -1,0 +1,78 @@
+"""Rank bodies of the multi-process (gloo, CPU) tests of sharded.py.  Each
+runs in a spawned process: it sets up its import path, joins the process
+group on 127.0.0.1 and writes its result to a .npz file."""
+import os
+import sys
+
+
+def _setup(root, rank, world, port):
+    for p in (os.path.join(root, "grn-gpu-performance_b200"), os.path.join(root, "oracle"),
+              os.path.join(root, "tests"), root):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    return dist
+
+
+class OracleEvaluator:
+    """evaluate_batch through the FP64 oracle (test stand-in for a GPU)."""
+
+    def __init__(self, sim, init, tgt):
+        self.sim, self.init, self.tgt = sim, init, tgt
+        self.seen = 0
+
+    def evaluate_batch(self, batch, max_error=None):
+        import binding as oracle
+        self.seen += batch.n_models
+        err, raw, steps = oracle.evaluate_batch(self.sim, self.init, self.tgt, batch, max_error,
+                                                n_threads=1)
+        return err, raw, {"n_models": batch.n_models}
+
+
+def sharded_eval(rank, world, port, root, out):
+    dist = _setup(root, rank, world, port)
+    import numpy as np
+    import synth
+    import sharded
+    params, batch, init, tgt = synth.workload("small_32x32", seed=21, n_models=23, steps=40,
+                                              W=12, H=10)
+    ev = OracleEvaluator(params, init, tgt)
+    me = np.linspace(0.05, 1000.0, batch.n_models)
+    sh = sharded.ShardedEvaluator(ev, params["n_input_morphogens"] +
+                                  params["n_target_morphogens"])
+    err, raw, _ = sh.evaluate_batch(batch, me)
+    np.savez(os.path.join(out, "rank%d.npz" % rank), err=err, raw=raw, seen=ev.seen)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def island_shards(rank, world, port, root, out):
+    dist = _setup(root, rank, world, port)
+    import numpy as np
+    import grn_b200 as grn
+    import synth
+    import sharded
+    sim = dict(dim_x=8, dim_y=8, n_input_morphogens=1, n_target_morphogens=1, num_sim_steps=20,
+               error_precision=6, fitness_kind=0, dt=0.1, min_conc=0.0, min_conc_change=1e-3,
+               dist_error_threshold=0.05)
+    wl = dict(synth.WORKLOADS["uneven_64x64"], W=8, H=8, n_exp=1)
+    init, tgt = synth.experiments(wl, 3)
+    ev = OracleEvaluator(sim, init, tgt)
+    evo = grn.Evolution(dict(n_demes=2, deme_size=8, migration_period=0, n_max_products=5,
+                             n_max_links=8, n_host_threads=1, seed=100 + rank), 2,
+                        calculator=lambda b, me: ev.evaluate_batch(b, me)[0])
+    isl = sharded.IslandShards(evo, 2, 8, period=2, seed=9)
+    stats = [isl.step() for _ in range(4)]
+    ex = isl.last_exchange
+    after = [evo.individual(ex["deme"], i) for i in ex["slots"]]
+    import pickle
+    with open(os.path.join(out, "rank%d.pkl" % rank), "wb") as f:
+        pickle.dump({"stats": stats, "after": after, "exchange": ex}, f)
+    evo.close()
+    dist.barrier()
+    dist.destroy_process_group()
