@@ -138,7 +138,11 @@ _SIGNATURES = {
     "grn_evolution_destroy": ([_P], _I),
     "grn_encode_models": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
     "grn_model_costs": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
+    "grn_model_format": ([_P, _I, _P, _I, _I, _P, _I, ctypes.POINTER(_I)], _I),
+    "grn_model_parse": ([ctypes.c_char_p, _P, _I, ctypes.POINTER(_I), _P, _I,
+                         ctypes.POINTER(_I)], _I),
     "grn_evolution_set_individual": ([_P, _I, _I, _P, _I, _P, _I, _D], _I),
+    "grn_evolution_set_generation": ([_P, _I], _I),
     "grn_surrogate_create": ([_I, ctypes.c_uint64, _I, ctypes.POINTER(_P)], _I),
     "grn_surrogate_destroy": ([_P], _I),
     "grn_surrogate_add_data": ([_P, _P, _P, _I], _I),
@@ -493,6 +497,9 @@ class Evolution:
             self.handle, deme, index, _ptr(p) if len(p) else None, len(p),
             _ptr(l) if len(l) else None, len(l), float(error)))
 
+    def set_generation(self, generation):
+        _check(self.lib.grn_evolution_set_generation(self.handle, generation))
+
     def set_skip_clones(self, enable=True):
         _check(self.lib.grn_evolution_set_skip_clones(self.handle, int(bool(enable))))
 
@@ -522,6 +529,36 @@ class Evolution:
 
 N_FEATURES = 128
 N_PARAMS = 164865
+
+
+def format_model(products, links, precision=6):
+    """grn_model_format: the reference's model string."""
+    lib = load_library()
+    p = np.ascontiguousarray(products, PRODUCT_DTYPE)
+    l = np.ascontiguousarray(links, LINK_DTYPE)
+    need = ctypes.c_int(0)
+    args = (_ptr(p) if len(p) else None, len(p), _ptr(l) if len(l) else None, len(l), precision)
+    st = lib.grn_model_format(*args, None, 0, ctypes.byref(need))
+    if st not in (0, 6):  # GRN_ERR_CAPACITY just reports the size
+        _check(st)
+    buf = ctypes.create_string_buffer(need.value)
+    _check(lib.grn_model_format(*args, buf, need.value, ctypes.byref(need)))
+    return buf.value.decode()
+
+
+def parse_model(text):
+    """grn_model_parse: (products, links) arrays of a model string."""
+    lib = load_library()
+    raw = text.encode()
+    npr, nli = ctypes.c_int(0), ctypes.c_int(0)
+    st = lib.grn_model_parse(raw, None, 0, ctypes.byref(npr), None, 0, ctypes.byref(nli))
+    if st not in (0, 6):
+        _check(st)
+    pr = np.zeros(npr.value, PRODUCT_DTYPE)
+    li = np.zeros(nli.value, LINK_DTYPE)
+    _check(lib.grn_model_parse(raw, _ptr(pr) if len(pr) else None, len(pr), ctypes.byref(npr),
+                               _ptr(li) if len(li) else None, len(li), ctypes.byref(nli)))
+    return pr, li
 
 
 def model_costs(batch, n_morphogens):

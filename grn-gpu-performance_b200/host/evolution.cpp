@@ -783,6 +783,18 @@ grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
   return GRN_OK;
 }
 
+grn_status grn_evolution_set_generation(grn_evolution *evo, int generation) {
+  if (!evo || generation < 0) return GRN_ERR_INVALID_ARGUMENT;
+  for (const auto &d : evo->demes)
+    for (const auto &ind : d.pop)
+      if (ind.model.prods.empty()) {
+        evo->last_error = "an individual has no model";
+        return GRN_ERR_MODEL;
+      }
+  evo->generation = generation;
+  return GRN_OK;
+}
+
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index) {
   if (!evo || !deme || !index || evo->generation < 0) return GRN_ERR_INVALID_ARGUMENT;
   double best = 1e300;

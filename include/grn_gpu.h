@@ -330,6 +330,21 @@ grn_status grn_describe_model(const grn_product *products, int n_products,
                               const grn_link *links, int n_links,
                               int n_morphogens, char *buf, int buf_len);
 
+/* ------------------------------------------------------- model text ---
+ * The reference's text form of a model (Model::toString / loadFromString,
+ * Src/Model/model.cpp:614-706):
+ *   "(" product ("|" product)* "*" [link ("|" link)*] ")"
+ *   product = "label init lim deg dif", link = "regulator regulated K n isAnd".
+ * grn_model_format writes doubles with `precision` significant digits (6 is
+ * the reference's QTextStream default; 17 round-trips exactly) and needs
+ * *needed bytes including the terminating 0 (GRN_ERR_CAPACITY if buf_len is
+ * smaller).  grn_model_parse returns GRN_ERR_MODEL for malformed text and
+ * GRN_ERR_CAPACITY (with the counts set) when the arrays are too small. */
+grn_status grn_model_format(const grn_product *products, int n_products, const grn_link *links,
+                            int n_links, int precision, char *buf, int buf_len, int *needed);
+grn_status grn_model_parse(const char *text, grn_product *products, int max_products,
+                           int *n_products, grn_link *links, int max_links, int *n_links);
+
 /* Relative simulation work of one cell-step of each model of a batch (host
  * only; the weights the evaluator uses to order its work queue), for
  * splitting a batch into equal-work shards across GPUs. */
@@ -403,6 +418,11 @@ grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int inde
 grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
                                         const grn_product *products, int n_products,
                                         const grn_link *links, int n_links, double error);
+/* Resumes a search whose populations were installed with
+ * grn_evolution_set_individual: the next grn_evolution_step reproduces from
+ * them (instead of creating random populations) as generation
+ * `generation` + 1.  GRN_ERR_MODEL if an individual has no model. */
+grn_status grn_evolution_set_generation(grn_evolution *evo, int generation);
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index);
 grn_status grn_evolution_destroy(grn_evolution *evo);
 
