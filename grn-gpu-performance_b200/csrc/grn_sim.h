@@ -43,6 +43,10 @@ struct SimArgs {
   float *state_out;          // optional final states
                              // [caller index][n_exp][state_planes][H][W]
   int32_t state_planes;
+  int32_t trace_every;       // steps between trace frames (frame 0: initial)
+  float *trace_out;          // optional trace frames [caller index][n_exp]
+                             // [trace_frames][state_planes][H][W]
+  int32_t trace_frames;
 };
 
 // One compiled kernel variant.
@@ -54,6 +58,7 @@ struct KernelVariant {
   bool ragged;  // compiled for W not a multiple of 4
   bool cluster; // cluster-split: a cluster of CTAs per model, one band of
                 // rows each
+  bool trace;   // writes trace frames (SimArgs::trace_out)
 };
 
 // Launch plan chosen by the host.

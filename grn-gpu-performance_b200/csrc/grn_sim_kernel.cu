@@ -555,6 +555,20 @@ __device__ __forceinline__ void push_halos(const SimArgs &A, const StatePtrs &sp
   }
 }
 
+// Copies the first min(G, A.state_planes) genes' current values of the
+// block's rows into dst ([plane][H][W], unpadded).
+template <int NT, int GMAX>
+__device__ __forceinline__ void write_planes(const SimArgs &A, const StatePtrs &sp, const Geom &g,
+                                          int G, int par, float *dst) {
+  const int planes_out = min(G, A.state_planes);
+  for (int i = threadIdx.x; i < planes_out * g.W * g.H; i += NT) {
+    const int kk = i / (g.W * g.H), r = i - kk * g.W * g.H;
+    const int y = r / g.W, x = r - y * g.W;
+    dst[((size_t)kk * g.Hg + g.y0 + y) * g.W + x] =
+        plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
+  }
+}
+
 // Cluster-wide combine of one value per CTA: CTA `rank` stores v into slot
 // `rank` of every CTA's array, then the cluster barrier (which also orders
 // the halo rows pushed before it).  Every CTA then reads the same C slots.
@@ -573,13 +587,15 @@ __device__ __forceinline__ void cluster_share(T *slots, T v, int rank, int C) {
 //   LOOP    grids with more groups than NT * ITEMS: each thread walks its
 //           groups with incrementally updated geometry
 //   RAGGED  W is not a multiple of 4
+//   TRACE   writes trace frames (trace_out) during the step loop; only the
+//           variants compiled for it carry that code
 //   CL      cluster-split: a cluster of C CTAs (launch attribute) simulates
 //           one model at a time, CTA r owning rows [r*Hb, r*Hb + Hb) with
 //           Hb = ceil(H / C).  Every CTA of a cluster takes the same branches
 //           and passes the same cluster barriers: the model index, the step
 //           max and the fitness sum are shared values, identical bits in
 //           every CTA.
-template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL>
+template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL, bool TRACE>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
@@ -706,6 +722,16 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       if constexpr (CL) cg::this_cluster().sync();
       else __syncthreads();
 
+      // Trace frames: the state after every trace_every-th step, frame 0
+      // the initial state.  A frame reads the current buffer while the
+      // next step writes the other one.
+      float *trace = nullptr;
+      if constexpr (TRACE) {
+        trace = A.trace_out + ((size_t)orig * A.n_exp + e) * A.trace_frames * A.state_planes *
+                                  g.W * g.Hg;
+        write_planes<NT, GMAX>(A, sp, g, G, 0, trace);
+      }
+
       double change = 1.0;
       int step = 0;
       int par = 0;  // buffer holding the current values
@@ -746,20 +772,19 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         change = (double)bm;
         par ^= 1;
         ++step;
+        if constexpr (TRACE) {
+          if (step % A.trace_every == 0 && step / A.trace_every < A.trace_frames)
+            write_planes<NT, GMAX>(A, sp, g, G, par,
+                                   trace + (size_t)(step / A.trace_every) * A.state_planes *
+                                               g.W * g.Hg);
+        }
       }
       steps_total += step;
       change_sum += change;
-      if (A.state_out) {
-        // Final state of this experiment, unpadded [gene][y][x].
-        const int planes_out = min(G, A.state_planes);
-        float *so = A.state_out + ((size_t)orig * A.n_exp + e) * A.state_planes * g.W * g.Hg;
-        for (int i = tid; i < planes_out * g.W * g.H; i += NT) {
-          const int kk = i / (g.W * g.H), r = i - kk * g.W * g.H;
-          const int y = r / g.W, x = r - y * g.W;
-          so[((size_t)kk * g.Hg + g.y0 + y) * g.W + x] =
-              plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
-        }
-      }
+      if (A.state_out)  // final state of this experiment, unpadded [gene][y][x]
+        write_planes<NT, GMAX>(A, sp, g, G, par,
+                               A.state_out + ((size_t)orig * A.n_exp + e) * A.state_planes *
+                                                 g.W * g.Hg);
 
       // Fitness of the experiment (simstate.cpp:135-158), FP64 sums.
       const float *tgt = A.target + (size_t)e * A.n_target * A.W * A.H;
@@ -809,9 +834,10 @@ struct VariantEntry {
   KernelFn fn;
 };
 
-#define GRN_VARIANT(NT, GMAX, ITEMS, LOOP, CL)                                         \
-  {{NT, GMAX, ITEMS, LOOP, false, CL}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL>},    \
-  {{NT, GMAX, ITEMS, LOOP, true, CL}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL>}
+#define GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, TR)                                      \
+  {{NT, GMAX, ITEMS, LOOP, false, CL, TR}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL, TR>}, \
+  {{NT, GMAX, ITEMS, LOOP, true, CL, TR}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL, TR>}
+#define GRN_VARIANT(NT, GMAX, ITEMS, LOOP, CL) GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, false)
 
 const VariantEntry kVariants[] = {
     GRN_VARIANT(256, 4, 1, false, false),  GRN_VARIANT(256, 8, 1, false, false),
@@ -820,8 +846,10 @@ const VariantEntry kVariants[] = {
     GRN_VARIANT(512, 8, 1, true, false),   GRN_VARIANT(512, 16, 1, true, false),
     GRN_VARIANT(256, 4, 1, true, false),
     // cluster-split
-    GRN_VARIANT(512, 8, 1, false, true),   GRN_VARIANT(512, 8, 2, false, true),
+    GRN_VARIANT(512, 8, 1, false, true),
     GRN_VARIANT(512, 8, 1, true, true),    GRN_VARIANT(512, 16, 1, true, true),
+    // trace frames (one model at a time: any grid, any gene count)
+    GRN_VARIANT_T(256, 16, 1, true, false, true),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -829,7 +857,8 @@ const VariantEntry *find_variant(const KernelVariant &v) {
   for (int i = 0; i < kNumVariants; ++i) {
     const KernelVariant &k = kVariants[i].v;
     if (k.threads == v.threads && k.gmax == v.gmax && k.items == v.items &&
-        k.loop == v.loop && k.ragged == v.ragged && k.cluster == v.cluster)
+        k.loop == v.loop && k.ragged == v.ragged && k.cluster == v.cluster &&
+        k.trace == v.trace)
       return &kVariants[i];
   }
   return nullptr;

@@ -138,6 +138,10 @@ _SIGNATURES = {
     "grn_evolution_destroy": ([_P], _I),
     "grn_encode_models": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
     "grn_model_costs": ([ctypes.POINTER(ModelBatchC), _I, _P], _I),
+    "grn_trace_model": ([_P, _P, _I, _P, _I, _I, _I, _I, _I, _P, ctypes.POINTER(_I), _P], _I),
+    "grn_render_cells": ([_P, _I, _I, _I, _I, _P], _I),
+    "grn_render_concentrations": ([_P, _I, _I, _I, _D, _P], _I),
+    "grn_write_ppm": ([ctypes.c_char_p, _P, _I, _I], _I),
     "grn_model_format": ([_P, _I, _P, _I, _I, _P, _I, ctypes.POINTER(_I)], _I),
     "grn_model_parse": ([ctypes.c_char_p, _P, _I, ctypes.POINTER(_I), _P, _I,
                          ctypes.POINTER(_I)], _I),
@@ -389,6 +393,20 @@ class Evaluator:
         err, raw, _, _ = self._keep.pop(tag.value)
         return tag.value, err, raw
 
+    def trace(self, products, links, experiment=0, every=1, max_frames=64, max_planes=16):
+        """grn_trace_model: (frames [n][planes][H][W], labels [planes])."""
+        p = np.ascontiguousarray(products, PRODUCT_DTYPE)
+        l = np.ascontiguousarray(links, LINK_DTYPE)
+        H, W = self.params["dim_y"], self.params["dim_x"]
+        frames = np.zeros((max_frames, max_planes, H, W), np.float32)
+        labels = np.zeros(max_planes, np.int32)
+        n = ctypes.c_int(0)
+        _check(self.lib.grn_trace_model(self.ctx, _ptr(p) if len(p) else None, len(p),
+                                        _ptr(l) if len(l) else None, len(l), experiment, every,
+                                        max_frames, max_planes, _ptr(frames), ctypes.byref(n),
+                                        _ptr(labels)), self.ctx)
+        return frames[:n.value], labels
+
     def pack(self, batch):
         return Packed(self, batch)
 
@@ -529,6 +547,30 @@ class Evolution:
 
 N_FEATURES = 128
 N_PARAMS = 164865
+
+
+def render_cells(planes, n_morphogens):
+    """grn_render_cells: [H][W][3] uint8 of planes [n][H][W]."""
+    p = np.ascontiguousarray(planes, np.float32)
+    out = np.zeros(p.shape[1:] + (3,), np.uint8)
+    _check(load_library().grn_render_cells(_ptr(p), p.shape[0], n_morphogens, p.shape[2],
+                                           p.shape[1], _ptr(out)))
+    return out
+
+
+def render_concentrations(planes, factor=1.0):
+    """grn_render_concentrations: [H][W][3] uint8 of planes [n][H][W]."""
+    p = np.ascontiguousarray(planes, np.float32)
+    out = np.zeros(p.shape[1:] + (3,), np.uint8)
+    _check(load_library().grn_render_concentrations(_ptr(p), p.shape[0], p.shape[2], p.shape[1],
+                                                    factor, _ptr(out)))
+    return out
+
+
+def write_ppm(path, rgb):
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    _check(load_library().grn_write_ppm(str(path).encode(), _ptr(rgb), rgb.shape[1],
+                                        rgb.shape[0]))
 
 
 def format_model(products, links, precision=6):

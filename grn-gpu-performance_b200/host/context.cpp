@@ -193,21 +193,22 @@ int host_threads() {
 // all-shared-memory state over state spilling to global slots.
 // Every feasible launch plan for a batch, with the heuristic throughput
 // score of each.
-grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models,
+grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace,
                            std::vector<std::pair<double, LaunchPlan>> *out) {
   const int W = ctx->p.dim_x, H = ctx->p.dim_y;
   const int Wg = (W + 3) / 4;
   const bool ragged = (W % 4) != 0;
   const size_t fixed = grn::sim_fixed_smem_bytes();
   const size_t optin = (size_t)ctx->smem_optin;
-  const int sched = ctx->forced_schedule;
+  // A trace runs on the trace variants whatever schedule is forced.
+  const int sched = trace ? GRN_SCHEDULE_WALK_ITEMS : ctx->forced_schedule;
   static const int kClusterSizes[] = {2, 4, 8, 16};
   out->clear();
   const int nv = grn::sim_variant_count();
   for (int i = 0; i < nv; ++i) {
     const grn::KernelVariant v = grn::sim_variant(i);
-    if (v.gmax < max_genes || v.ragged != ragged) continue;
-    if (ctx->forced_threads && v.threads != ctx->forced_threads) continue;
+    if (v.gmax < max_genes || v.ragged != ragged || v.trace != trace) continue;
+    if (ctx->forced_threads && !trace && v.threads != ctx->forced_threads) continue;
     if (sched == GRN_SCHEDULE_CLUSTER && !v.cluster) continue;
     if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_CLUSTER && v.cluster) continue;
     if (sched == GRN_SCHEDULE_FIXED_ITEMS && v.loop) continue;
@@ -283,7 +284,7 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models,
 
 grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *out) {
   std::vector<std::pair<double, LaunchPlan>> plans;
-  grn_status s = enumerate_plans(ctx, max_genes, n_models, &plans);
+  grn_status s = enumerate_plans(ctx, max_genes, n_models, false, &plans);
   if (s != GRN_OK) return s;
   *out = plans[0].second;
   return GRN_OK;
@@ -365,17 +366,27 @@ grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, Launc
   return GRN_OK;
 }
 
+// Optional outputs of a launch: final states, trace frames, one experiment.
+struct LaunchExtras {
+  float *states = nullptr;  // [model][n_exp][state_planes][H][W]
+  int state_planes = 0;
+  float *trace = nullptr;   // [model][n_exp][trace_frames][state_planes][H][W]
+  int trace_every = 0, trace_frames = 0;
+  int experiment = -1;      // >= 0: simulate only this experiment
+};
+
 // Launches the simulation of `n_models` packed records already on the
 // device.  `stream` may differ from the context's stream.
 grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
                          int n_models, int max_genes, int max_links,
                          const double *d_max_error, double *d_raw, int32_t *d_steps,
                          int32_t *d_flag, cudaStream_t stream, LaunchPlan *plan_out,
-                         float *d_states = nullptr, int state_planes = 0) {
+                         const LaunchExtras &ex = LaunchExtras()) {
   if (n_models == 0) return GRN_OK;
   if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
+  const bool trace = ex.trace != nullptr;
   std::vector<std::pair<double, LaunchPlan>> plans;
-  grn_status s = enumerate_plans(ctx, max_genes, n_models, &plans);
+  grn_status s = enumerate_plans(ctx, max_genes, n_models, trace, &plans);
   if (s != GRN_OK) return s;
   LaunchPlan plan = plans[0].second;
   const int W = ctx->p.dim_x, H = ctx->p.dim_y, Wg = (W + 3) / 4;
@@ -403,10 +414,19 @@ grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_of
   a.steps = d_steps;
   a.work_counter = static_cast<int32_t *>(ctx->d_counter.p);
   a.error_flag = d_flag;
-  a.state_out = d_states;
-  a.state_planes = state_planes;
+  a.state_out = ex.states;
+  a.state_planes = ex.state_planes;
+  a.trace_out = ex.trace;
+  a.trace_every = ex.trace_every;
+  a.trace_frames = ex.trace_frames;
   a.fast_ok = ctx->fast_ok ? 1 : 0;
-  if (ctx->forced_schedule == GRN_SCHEDULE_AUTO && ctx->autotune && plans.size() > 1) {
+  if (ex.experiment >= 0) {
+    const size_t cells = (size_t)W * H;
+    a.initial += (size_t)ex.experiment * a.n_in * cells;
+    a.target += (size_t)ex.experiment * a.n_target * cells;
+    a.n_exp = 1;
+  }
+  if (!trace && ctx->forced_schedule == GRN_SCHEDULE_AUTO && ctx->autotune && plans.size() > 1) {
     const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
     const std::array<int, 7> key = {W, H, max_genes, max_links, ctx->n_exp,
                                     ctx->fast_ok ? 1 : 0, bucket};
@@ -751,7 +771,12 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
                       static_cast<const int32_t *>(j.d_offsets.p), n, ph.max_genes, ph.max_links,
                       static_cast<const double *>(j.d_maxerr.p), static_cast<double *>(j.d_raw.p),
                       static_cast<int32_t *>(j.d_steps.p), static_cast<int32_t *>(j.d_flag.p), st,
-                      nullptr, static_cast<float *>(d_states.p), max_planes);
+                      nullptr, [&] {
+                        LaunchExtras x;
+                        x.states = static_cast<float *>(d_states.p);
+                        x.state_planes = max_planes;
+                        return x;
+                      }());
     int32_t flag = 0;
     chk(cudaMemcpyAsync(states_out, d_states.p, sb, cudaMemcpyDeviceToHost, st));
     if (raw_error_out) chk(cudaMemcpyAsync(raw_error_out, j.d_raw.p, eb, cudaMemcpyDeviceToHost, st));
@@ -899,6 +924,80 @@ grn_status grn_packed_get_info(const grn_packed *pk, grn_packed_info *info) {
   return GRN_OK;
 }
 
+grn_status grn_trace_model(grn_ctx *ctx, const grn_product *products, int n_products,
+                           const grn_link *links, int n_links, int experiment, int every,
+                           int max_frames, int max_planes, float *frames_out, int *n_frames,
+                           int32_t *labels_out) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (n_products < 0 || n_links < 0 || (n_products && !products) || (n_links && !links) ||
+      every < 1 || max_frames < 1 || max_planes < 1 || !frames_out || !n_frames)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad trace arguments");
+  if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
+  if (experiment < 0 || experiment >= ctx->n_exp)
+    return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "no such experiment");
+  cudaSetDevice(ctx->device);
+  const int n_morph = ctx->p.n_input_morphogens + ctx->p.n_target_morphogens;
+  int32_t po[2] = {0, n_products}, lo[2] = {0, n_links};
+  grn_model_batch b{};
+  b.n_models = 1;
+  b.product_offsets = po;
+  b.products = products;
+  b.link_offsets = lo;
+  b.links = links;
+  PackedHost ph;
+  std::string err;
+  grn_status s = grn::pack_batch(&b, n_morph, 1, &ph, &err);
+  if (s != GRN_OK) return fail(ctx, s, err);
+  const size_t cells = (size_t)ctx->p.dim_x * ctx->p.dim_y;
+  const size_t fb = (size_t)max_frames * max_planes * cells * sizeof(float);
+  Job &j = ctx->sync_job;
+  DevBuf d_trace;
+  const size_t wb = ph.words.size() * sizeof(uint4);
+  if ((s = ensure_dev(ctx, &j.d_words, wb)) || (s = ensure_dev(ctx, &j.d_offsets, 4)) ||
+      (s = ensure_dev(ctx, &j.d_maxerr, 8)) || (s = ensure_dev(ctx, &j.d_raw, 8)) ||
+      (s = ensure_dev(ctx, &j.d_steps, 4)) || (s = ensure_dev(ctx, &j.d_flag, 4)) ||
+      (s = ensure_dev(ctx, &d_trace, fb)))
+    return s;
+  cudaStream_t st = ctx->stream;
+  const double never = 1e300;  // no abandon
+  int32_t steps = 0, flag = 0;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(cudaMemcpyAsync(j.d_words.p, ph.words.data(), wb, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j.d_offsets.p, ph.offsets.data(), 4, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j.d_maxerr.p, &never, 8, cudaMemcpyHostToDevice, st));
+  chk(cudaMemsetAsync(j.d_flag.p, 0, 4, st));
+  chk(cudaMemsetAsync(d_trace.p, 0, fb, st));
+  if (e == cudaSuccess) {
+    LaunchExtras x;
+    x.state_planes = max_planes;
+    x.trace = static_cast<float *>(d_trace.p);
+    x.trace_every = every;
+    x.trace_frames = max_frames;
+    x.experiment = experiment;
+    s = launch_packed(ctx, static_cast<const uint4 *>(j.d_words.p),
+                      static_cast<const int32_t *>(j.d_offsets.p), 1, ph.max_genes, ph.max_links,
+                      static_cast<const double *>(j.d_maxerr.p), static_cast<double *>(j.d_raw.p),
+                      static_cast<int32_t *>(j.d_steps.p), static_cast<int32_t *>(j.d_flag.p), st,
+                      nullptr, x);
+    chk(cudaMemcpyAsync(frames_out, d_trace.p, fb, cudaMemcpyDeviceToHost, st));
+    chk(cudaMemcpyAsync(&steps, j.d_steps.p, 4, cudaMemcpyDeviceToHost, st));
+    chk(cudaMemcpyAsync(&flag, j.d_flag.p, 4, cudaMemcpyDeviceToHost, st));
+    chk(cudaStreamSynchronize(st));
+  }
+  cudaFree(d_trace.p);
+  if (s != GRN_OK) return s;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "trace");
+  if (flag) return fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected the model");
+  *n_frames = std::min(max_frames, steps / every + 1);
+  if (labels_out) {
+    const std::vector<int> labels = grn::labels_in_use(links, n_links, n_morph);
+    for (int i = 0; i < max_planes; ++i)
+      labels_out[i] = i < (int)labels.size() ? labels[i] : -1;
+  }
+  return GRN_OK;
+}
+
 grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_max_error,
                           double *d_raw_error, int32_t *d_steps, void *cuda_stream) {
   if (!ctx || !pk || pk->ctx != ctx) return GRN_ERR_INVALID_ARGUMENT;
@@ -956,15 +1055,7 @@ extern "C" grn_status grn_describe_model(const grn_product *products, int n_prod
   std::snprintf(line, sizeof line, "model genes %d links %d lg_mask %u\n", hdr.n_genes,
                 hdr.n_links, hdr.lg_mask);
   out += line;
-  // Labels are the sorted labels in use; recompute them for the listing.
-  std::vector<int> labels;
-  for (int i = 0; i < n_morphogens; ++i) labels.push_back(i);
-  for (size_t h = 0; h < labels.size(); ++h)
-    for (int l = 0; l < n_links; ++l)
-      if (links[l].regulated == labels[h] &&
-          std::find(labels.begin(), labels.end(), links[l].regulator) == labels.end())
-        labels.push_back(links[l].regulator);
-  std::sort(labels.begin(), labels.end());
+  const std::vector<int> labels = grn::labels_in_use(links, n_links, n_morphogens);
   for (int i = 0; i < hdr.n_genes; ++i) {
     grn::PackedGene g;
     std::memcpy(&g, rec.data() + 1 + i, sizeof g);

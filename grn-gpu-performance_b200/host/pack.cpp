@@ -18,6 +18,17 @@ bool contains(const std::vector<int> &v, int x) {
 
 }  // namespace
 
+std::vector<int> labels_in_use(const grn_link *links, int n_links, int n_morphogens) {
+  std::vector<int> labels;
+  for (int i = 0; i < n_morphogens; ++i) labels.push_back(i);
+  for (size_t h = 0; h < labels.size(); ++h)
+    for (int l = 0; l < n_links; ++l)
+      if (links[l].regulated == labels[h] && !contains(labels, links[l].regulator))
+        labels.push_back(links[l].regulator);
+  std::sort(labels.begin(), labels.end());
+  return labels;
+}
+
 grn_status pack_model(const grn_product *products, int n_products,
                       const grn_link *links, int n_links, int n_morphogens,
                       int orig_index, std::vector<uint4> *out,

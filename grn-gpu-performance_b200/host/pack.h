@@ -31,6 +31,11 @@ grn_status pack_model(const grn_product *products, int n_products,
                       int orig_index, std::vector<uint4> *out,
                       ModelCost *cost, std::string *err);
 
+// Sorted labels in use: the morphogens and, transitively, their regulators
+// (Model::calcProductLabelsInUse, Src/Model/model.cpp:243-270); the order of
+// a compiled model's genes.
+std::vector<int> labels_in_use(const grn_link *links, int n_links, int n_morphogens);
+
 // A whole batch, records ordered by decreasing cost so that the persistent
 // kernel's work queue hands out the longest models first.
 struct PackedHost {

@@ -330,6 +330,34 @@ grn_status grn_describe_model(const grn_product *products, int n_products,
                               const grn_link *links, int n_links,
                               int n_morphogens, char *buf, int buf_len);
 
+/* ------------------------------------------------- headless viewer ---
+ * Replaces the reference viewer's simulation thread and its image threads
+ * (Src/UI/GUICommon/Simulator/simulatorthread.cpp:30-59,
+ * cellimagethread.cpp, concentimagethread.cpp) without a display. */
+
+/* Simulates one model on experiment `experiment` and records its state
+ * every `every` Euler steps: frames_out [max_frames][max_planes][dim_y][dim_x]
+ * (frame 0 the initial state, frame f the state after f * every steps;
+ * plane p the p-th product in use, zero past the model's products).
+ * *n_frames = frames written (the simulation may stop early); labels_out
+ * (optional, [max_planes]) the plane's product label or -1. */
+grn_status grn_trace_model(grn_ctx *ctx, const grn_product *products, int n_products,
+                           const grn_link *links, int n_links, int experiment, int every,
+                           int max_frames, int max_planes, float *frames_out, int *n_frames,
+                           int32_t *labels_out);
+
+/* The viewer's cell image of a state (planes [n_planes][height][width], the
+ * products in use in label order): morphogens 0..2 as red, green, blue,
+ * 255 * min(1, c).  rgb: [height][width][3]. */
+grn_status grn_render_cells(const float *planes, int n_planes, int n_morphogens, int width,
+                            int height, uint8_t *rgb);
+/* The viewer's concentration image: every product adds its palette colour
+ * times c / factor, clamped at 255. */
+grn_status grn_render_concentrations(const float *planes, int n_planes, int width, int height,
+                                     double factor, uint8_t *rgb);
+/* Writes rgb [height][width][3] as a binary PPM (P6) file. */
+grn_status grn_write_ppm(const char *path, const uint8_t *rgb, int width, int height);
+
 /* ------------------------------------------------------- model text ---
  * The reference's text form of a model (Model::toString / loadFromString,
  * Src/Model/model.cpp:614-706):

@@ -255,6 +255,41 @@ def test_cluster_schedule_rejects_empty_bands():
         assert "CAPACITY" in str(e.value)
 
 
+def test_trace_frames_match_shorter_runs():
+    """Frame f of a trace is the state after f * every steps: bitwise the
+    final state of the same model simulated for that many steps."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=19, n_models=3, steps=30,
+                                              W=20, H=14, n_exp=2)
+    every, n_frames = 7, 5
+    prods, links = batch.model(1)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        frames, labels = ev.trace(prods, links, experiment=1, every=every,
+                                  max_frames=n_frames, max_planes=8)
+    assert frames.shape == (n_frames, 8, 14, 20)
+    assert labels[0] == 0 and (np.diff(labels[labels >= 0]) > 0).all()
+    np.testing.assert_array_equal(frames[0, 0], init[1, 0].astype(np.float32))
+    assert not frames[0, 1:].any()  # products other than the input start at 0
+    one = grn.ModelBatch.from_models([(prods, links)])
+    for f in range(1, n_frames):
+        p = dict(params, num_sim_steps=f * every)
+        with grn.Evaluator(p) as ev:
+            ev.set_experiments(init, tgt)
+            _, states = ev.evaluate_states(one, max_planes=8)
+        np.testing.assert_array_equal(frames[f], states[0, 1], err_msg="frame %d" % f)
+
+
+def test_trace_stops_with_the_simulation():
+    params, batch, init, tgt = synth.workload("small_32x32", seed=20, n_models=1, steps=4000,
+                                              min_conc_change=1e-2, fitness=0)
+    prods, links = batch.model(0)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        _, _, st = ev.evaluate_batch(batch)
+        frames, _ = ev.trace(prods, links, every=10, max_frames=1000, max_planes=4)
+    assert len(frames) == st["total_steps"] // 10 + 1 < 1000
+
+
 def test_early_exit_and_steps():
     """minConcChange stops simulations early; the non-convergence penalty
     uses the running change sum."""
