@@ -147,6 +147,7 @@ _SIGNATURES = {
                          ctypes.POINTER(_I)], _I),
     "grn_evolution_set_individual": ([_P, _I, _I, _P, _I, _P, _I, _D], _I),
     "grn_evolution_set_generation": ([_P, _I], _I),
+    "grn_evolution_set_pipeline": ([_P, _I], _I),
     "grn_surrogate_create": ([_I, ctypes.c_uint64, _I, ctypes.POINTER(_P)], _I),
     "grn_surrogate_destroy": ([_P], _I),
     "grn_surrogate_add_data": ([_P, _P, _P, _I], _I),
@@ -514,6 +515,9 @@ class Evolution:
         _check(self.lib.grn_evolution_set_individual(
             self.handle, deme, index, _ptr(p) if len(p) else None, len(p),
             _ptr(l) if len(l) else None, len(l), float(error)))
+
+    def set_pipeline(self, enable=True):
+        _check(self.lib.grn_evolution_set_pipeline(self.handle, int(bool(enable))))
 
     def set_generation(self, generation):
         _check(self.lib.grn_evolution_set_generation(self.handle, generation))

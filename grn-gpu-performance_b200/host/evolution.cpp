@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <thread>
@@ -337,6 +338,10 @@ struct Deme {
 
 }  // namespace
 
+namespace {
+struct Flight;  // one half of the demes' children in evaluation (pipelined mode)
+}  // namespace
+
 struct grn_evolution {
   grn_evolution_params p{};
   grn::ModelOps ops{};
@@ -352,6 +357,11 @@ struct grn_evolution {
   grn::Rng search_rng{0};
   int generation = -1;
   std::string last_error;
+  // Pipelined mode: demes [0, n/2) and [n/2, n) alternate on the GPU.
+  bool pipelined = false;
+  bool primed = false;  // both halves' children are in flight
+  std::unique_ptr<Flight> flights[2];
+  ~grn_evolution();
 };
 
 namespace {
@@ -586,6 +596,140 @@ double ms_since(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
 
+// Children of one half of the demes submitted to the GPU evaluator; the
+// result arrays stay here until grn_wait_any returns the half's tag.
+struct Flight {
+  std::vector<Individual *> sim;
+  std::unique_ptr<FlatBatch> fb;
+  std::vector<double> max_err, err, raw;
+  int n_clones = 0;  // children accepted as clones of their parent
+  bool active = false;
+};
+
+constexpr int kFlightTag = 0x47524e00;  // tags kFlightTag + half
+
+void half_range(const grn_evolution *evo, int half, int *d0, int *d1) {
+  const int n = (int)evo->demes.size(), mid = n / 2;
+  *d0 = half == 0 ? 0 : mid;
+  *d1 = half == 0 ? mid : n;
+}
+
+// Reproduces the demes of one half (with clone acceptance) and submits the
+// children that need simulating.
+grn_status launch_half(grn_evolution *evo, int half, grn_generation_stats *st) {
+  int d0, d1;
+  half_range(evo, half, &d0, &d1);
+  Flight &f = *evo->flights[half];
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  const int nt = std::max(1, std::min(d1 - d0, evo->p.n_host_threads > 0
+                                                   ? evo->p.n_host_threads
+                                                   : (int)std::thread::hardware_concurrency()));
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int d = d0 + t; d < d1; d += nt) {
+        Deme &dm = evo->demes[d];
+        reproduce(evo, dm);
+        if (!evo->skip_clones) continue;
+        for (size_t i = 0; i < dm.children.size(); ++i) {
+          Individual &c = dm.children[i];
+          const Individual &p = dm.pop[dm.perm[i]];
+          c.clone = p.error < 100 && same_key(program_key(c.model, evo->ops.n_morph),
+                                              program_key(p.model, evo->ops.n_morph));
+          if (c.clone) c.error = p.error;
+        }
+      }
+    });
+  for (auto &th : pool) th.join();
+  f.sim.clear();
+  f.n_clones = 0;
+  for (int d = d0; d < d1; ++d)
+    for (auto &ind : evo->demes[d].children) {
+      if (ind.clone) f.n_clones += 1;
+      else f.sim.push_back(&ind);
+    }
+  f.fb.reset(new FlatBatch(f.sim));
+  f.max_err.clear();
+  for (Individual *ind : f.sim) f.max_err.push_back(ind->parent_error);
+  f.err.assign(f.sim.size(), 0.0);
+  f.raw.assign(f.sim.size(), 0.0);
+  st->host_ms += ms_since(t0);
+  const grn_status s = grn_submit(evo->ctx, kFlightTag + half, &f.fb->b, f.max_err.data(),
+                                  f.err.data(), f.raw.data());
+  if (s != GRN_OK) return s;
+  f.active = true;
+  return GRN_OK;
+}
+
+// Waits until the half's batch has been evaluated (results in its arrays).
+grn_status wait_half(grn_evolution *evo, int half, grn_generation_stats *st) {
+  auto t0 = std::chrono::steady_clock::now();
+  while (evo->flights[half]->active) {
+    int tag = -1;
+    const grn_status s = grn_wait_any(evo->ctx, -1, &tag);
+    if (s != GRN_OK) return s;
+    if (tag == kFlightTag || tag == kFlightTag + 1) evo->flights[tag - kFlightTag]->active = false;
+  }
+  if (st) st->eval_ms += ms_since(t0);
+  return GRN_OK;
+}
+
+void settle_half(grn_evolution *evo, int half, grn_generation_stats *st) {
+  auto t0 = std::chrono::steady_clock::now();
+  Flight &f = *evo->flights[half];
+  for (size_t i = 0; i < f.sim.size(); ++i) f.sim[i]->error = f.err[i];
+  st->n_evaluated += (int32_t)f.sim.size();
+  st->n_clones += f.n_clones;
+  int d0, d1;
+  half_range(evo, half, &d0, &d1);
+  for (int d = d0; d < d1; ++d) choose_next(evo->demes[d]);
+  st->host_ms += ms_since(t0);
+}
+
+// Drops the children in flight (their parents stay); used before the
+// populations are replaced from outside.
+grn_status drain(grn_evolution *evo) {
+  if (!evo->primed) return GRN_OK;
+  for (int h = 0; h < 2; ++h) {
+    const grn_status s = wait_half(evo, h, nullptr);
+    if (s != GRN_OK) return s;
+  }
+  for (auto &d : evo->demes) d.children.clear();
+  evo->primed = false;
+  return GRN_OK;
+}
+
+// One generation with the halves' evaluations overlapping the host work:
+//   wait half 0, select it, reproduce + submit it (the GPU runs half 1);
+//   wait half 1, select it, migrate if due, reproduce + submit half 1
+//   (half 0 first if migration held it back).
+// The sequence of reproductions, selections and migrations of every deme
+// is the synchronous mode's, so the populations are identical.
+grn_status pipelined_step(grn_evolution *evo, grn_generation_stats *st) {
+  if (!evo->primed) {
+    for (int h = 0; h < 2; ++h) {
+      const grn_status s = launch_half(evo, h, st);
+      if (s != GRN_OK) return s;
+    }
+    evo->primed = true;
+  }
+  const bool migrate_now = evo->p.migration_period > 0 && evo->demes.size() > 1 &&
+                           (evo->generation + 1) % evo->p.migration_period == 0;
+  grn_status s = wait_half(evo, 0, st);
+  if (s != GRN_OK) return s;
+  settle_half(evo, 0, st);
+  if (!migrate_now && (s = launch_half(evo, 0, st)) != GRN_OK) return s;
+  if ((s = wait_half(evo, 1, st)) != GRN_OK) return s;
+  settle_half(evo, 1, st);
+  evo->generation += 1;
+  if (migrate_now) {
+    migrate(evo);
+    st->migrated = 1;
+    if ((s = launch_half(evo, 0, st)) != GRN_OK) return s;
+  }
+  return launch_half(evo, 1, st);
+}
+
 }  // namespace
 
 extern "C" {
@@ -636,7 +780,8 @@ grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
                                        double simulate_fraction, int min_train_pairs,
                                        int batches_per_generation, int batch_size, float lr) {
   if (!evo || (s && (!(simulate_fraction > 0) || simulate_fraction > 1 || min_train_pairs < 1 ||
-                     batches_per_generation < 0 || batch_size < 1 || !(lr > 0))))
+                     batches_per_generation < 0 || batch_size < 1 || !(lr > 0) ||
+                     evo->pipelined)))
     return GRN_ERR_INVALID_ARGUMENT;
   evo->sur = s;
   evo->sim_fraction = simulate_fraction;
@@ -647,9 +792,40 @@ grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
   return GRN_OK;
 }
 
+grn_evolution::~grn_evolution() {
+  if (primed) drain(this);
+}
+
+grn_status grn_evolution_set_pipeline(grn_evolution *evo, int enable) {
+  if (!evo) return GRN_ERR_INVALID_ARGUMENT;
+  if (enable && (!evo->ctx || evo->sur || evo->demes.size() < 2)) {
+    evo->last_error = "pipelining needs the GPU evaluator, no surrogate and two or more demes";
+    return GRN_ERR_INVALID_ARGUMENT;
+  }
+  if (!enable) {
+    const grn_status s = drain(evo);
+    if (s != GRN_OK) return s;
+  }
+  for (auto &f : evo->flights)
+    if (!f) f.reset(new Flight());
+  evo->pipelined = enable != 0;
+  return GRN_OK;
+}
+
 grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
   if (!evo) return GRN_ERR_INVALID_ARGUMENT;
   grn_generation_stats st{};
+  if (evo->pipelined && evo->generation >= 0) {
+    const grn_status s = pipelined_step(evo, &st);
+    if (s != GRN_OK) {
+      evo->last_error = "pipelined generation failed";
+      return s;
+    }
+    st.generation = evo->generation;
+    fill_stats(evo, &st);
+    if (stats) *stats = st;
+    return GRN_OK;
+  }
   auto t0 = std::chrono::steady_clock::now();
   std::vector<Individual *> todo;
   if (evo->generation < 0) {
@@ -775,6 +951,9 @@ grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
       index >= (int)evo->demes[deme].pop.size() || n_products < 0 || n_links < 0 ||
       (n_products && !products) || (n_links && !links))
     return GRN_ERR_INVALID_ARGUMENT;
+  // Children in flight were bred from the populations being changed.
+  const grn_status ds = drain(evo);
+  if (ds != GRN_OK) return ds;
   Individual &ind = evo->demes[deme].pop[index];
   ind.model.prods.assign(products, products + n_products);
   ind.model.links.assign(links, links + n_links);
@@ -785,6 +964,8 @@ grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
 
 grn_status grn_evolution_set_generation(grn_evolution *evo, int generation) {
   if (!evo || generation < 0) return GRN_ERR_INVALID_ARGUMENT;
+  const grn_status ds = drain(evo);
+  if (ds != GRN_OK) return ds;
   for (const auto &d : evo->demes)
     for (const auto &ind : d.pop)
       if (ind.model.prods.empty()) {

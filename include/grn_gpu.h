@@ -446,6 +446,19 @@ grn_status grn_evolution_individual(const grn_evolution *evo, int deme, int inde
 grn_status grn_evolution_set_individual(grn_evolution *evo, int deme, int index,
                                         const grn_product *products, int n_products,
                                         const grn_link *links, int n_links, double error);
+/* Pipelined generations (GPU evaluator only, no surrogate, two or more
+ * demes): the demes split into two halves whose evaluations alternate on the
+ * GPU, each half's selection and reproduction running on the host while the
+ * other half is simulated -- the overlap the reference gets from its
+ * asynchronous per-deme loop (Search::calcParalEvolution,
+ * Src/Search/search.cpp:132-213, with ErrorCalculator::waitForAnyDeme).
+ * Every deme sees the same reproductions, selections and migrations as in
+ * the synchronous mode, so the populations are identical; the next
+ * generation's children are bred at the end of a step.  Changing a
+ * population (grn_evolution_set_individual / _set_generation) first drops
+ * the children in flight.  Destroy the search before its evaluator. */
+grn_status grn_evolution_set_pipeline(grn_evolution *evo, int enable);
+
 /* Resumes a search whose populations were installed with
  * grn_evolution_set_individual: the next grn_evolution_step reproduces from
  * them (instead of creating random populations) as generation

@@ -151,3 +151,40 @@ def test_evolution_on_gpu_matches_oracle_errors():
     errs = np.array(errs)
     ok = (np.abs(errs - oe) <= 1e-7 + 1e-4 * np.abs(oe)) | (errs == 100.0)
     assert ok.all(), (errs[~ok], oe[~ok])
+
+
+def test_pipeline_needs_gpu_evaluator(built_libs):
+    evo = grn.Evolution(EVO, 2, calculator=OracleCalculator(SIM))
+    with pytest.raises(grn.GrnError):
+        evo.set_pipeline(True)
+    evo.close()
+
+
+@pytest.mark.gpu
+def test_pipelined_generations_match_synchronous():
+    """Two halves of the demes alternating on the GPU while the host breeds
+    the other half: the same populations as the synchronous search."""
+    sim = dict(SIM, dim_x=16, dim_y=16, num_sim_steps=60)
+    init, tgt = _experiments(sim)
+    runs = []
+    for pipe in (False, True):
+        with grn.Evaluator(sim) as ev:
+            ev.set_experiments(init, tgt)
+            evo = grn.Evolution(dict(EVO, deme_size=32, n_max_products=8, n_max_links=24,
+                                     migration_period=3, seed=31), 2, evaluator=ev)
+            evo.set_skip_clones(True)
+            if pipe:
+                evo.set_pipeline(True)
+            st = [evo.step() for _ in range(8)]
+            models = [evo.individual(d, i) for d in range(4) for i in range(32)]
+            if pipe:  # replacing an individual drops the children in flight
+                p, l, e, _ = models[5]
+                evo.set_individual(0, 0, p, l, e)
+                evo.step()
+            evo.close()
+        runs.append((st, models))
+    (s1, m1), (s2, m2) = runs
+    for k in ("generation", "best_error", "mean_error", "n_evaluated", "n_clones", "migrated"):
+        assert [x[k] for x in s1] == [x[k] for x in s2], k
+    for a, b in zip(m1, m2):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
