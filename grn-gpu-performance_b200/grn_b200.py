@@ -114,6 +114,7 @@ _SIGNATURES = {
     "grn_set_schedule": ([_P, _I, _I], _I),
     "grn_set_cluster_size": ([_P, _I], _I),
     "grn_set_autotune": ([_P, _I], _I),
+    "grn_set_graphs": ([_P, _I], _I),
     "grn_set_experiments": ([_P, _I, _P, _P], _I),
     "grn_set_experiments_rgb": ([_P, _I, _P, _P], _I),
     "grn_decode_rgb": ([_I, _I, _I, _P, _P], _I),
@@ -324,6 +325,9 @@ class Evaluator:
     def set_schedule(self, schedule, threads=0, cluster_size=0):
         _check(self.lib.grn_set_schedule(self.ctx, schedule, threads), self.ctx)
         _check(self.lib.grn_set_cluster_size(self.ctx, cluster_size), self.ctx)
+
+    def set_graphs(self, enable=True):
+        _check(self.lib.grn_set_graphs(self.ctx, int(bool(enable))), self.ctx)
 
     def set_autotune(self, enable=True):
         _check(self.lib.grn_set_autotune(self.ctx, int(bool(enable))), self.ctx)

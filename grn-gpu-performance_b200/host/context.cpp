@@ -47,6 +47,7 @@ struct Job {
   DevBuf d_words, d_offsets, d_maxerr, d_raw, d_steps, d_flag;
   HostBuf h_words, h_offsets, h_maxerr, h_raw, h_steps, h_flag;
   cudaEvent_t ev_start = nullptr, ev_kernel = nullptr, ev_done = nullptr;
+  cudaGraphExec_t exec = nullptr;  // graph mode: this job's instantiated graph
   // Results of an asynchronous submission.
   int tag = 0;
   int n_models = 0;
@@ -73,6 +74,7 @@ struct grn_ctx {
   int forced_schedule = GRN_SCHEDULE_AUTO;
   int forced_threads = 0;
   int forced_cluster = 0;
+  bool graphs = false;  // evaluations replay one CUDA graph per job
   // Measured autotuning of GRN_SCHEDULE_AUTO: the fastest plan timed on a
   // sample of the first batch of each shape, by (W, H, max genes, max links,
   // experiments, fast path, batch-size bucket).
@@ -143,6 +145,7 @@ void free_job(Job *j) {
     if (b->p) cudaFreeHost(b->p);
   for (cudaEvent_t e : {j->ev_start, j->ev_kernel, j->ev_done})
     if (e) cudaEventDestroy(e);
+  if (j->exec) cudaGraphExecDestroy(j->exec);
 }
 
 grn_status check_params(const grn_sim_params *p) {
@@ -298,20 +301,35 @@ bool same_plan(const LaunchPlan &a, const grn::KernelVariant &v, int cluster, in
 
 // Launches the simulation of `n_models` packed records already on the
 // device.  `stream` may differ from the context's stream.
-grn_status launch_plan(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs a, cudaStream_t stream) {
-  a.planes = plan.planes;
-  a.gstate = nullptr;
-  a.slot_floats = 0;
+// Sets the plan's state planes and global state slots in `a` (allocating
+// the slots if they grew).
+grn_status bind_state(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs *a) {
+  a->planes = plan.planes;
+  a->gstate = nullptr;
+  a->slot_floats = 0;
   if (plan.slot_floats > 0) {
     grn_status s =
         ensure_dev(ctx, &ctx->d_gstate, (size_t)plan.slot_floats * plan.blocks * sizeof(float));
     if (s != GRN_OK) return s;
-    a.gstate = static_cast<float *>(ctx->d_gstate.p);
-    a.slot_floats = plan.slot_floats;
+    a->gstate = static_cast<float *>(ctx->d_gstate.p);
+    a->slot_floats = plan.slot_floats;
   }
+  return GRN_OK;
+}
+
+// Enqueues one launch whose arguments bind_state has completed: the work
+// counter reset and the kernel (no allocation, no synchronisation).
+grn_status enqueue_plan(grn_ctx *ctx, const LaunchPlan &plan, const grn::SimArgs &a,
+                        cudaStream_t stream) {
   GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter.p, 0, sizeof(int32_t), stream));
   GRN_CUDA(ctx, grn::sim_launch(plan, a, stream));
   return GRN_OK;
+}
+
+grn_status launch_plan(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs a, cudaStream_t stream) {
+  grn_status s = bind_state(ctx, plan, &a);
+  if (s != GRN_OK) return s;
+  return enqueue_plan(ctx, plan, a, stream);
 }
 
 // Measured autotuning: times the feasible plans (best heuristic scores
@@ -375,14 +393,15 @@ struct LaunchExtras {
   int experiment = -1;      // >= 0: simulate only this experiment
 };
 
-// Launches the simulation of `n_models` packed records already on the
-// device.  `stream` may differ from the context's stream.
-grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
-                         int n_models, int max_genes, int max_links,
-                         const double *d_max_error, double *d_raw, int32_t *d_steps,
-                         int32_t *d_flag, cudaStream_t stream, LaunchPlan *plan_out,
-                         const LaunchExtras &ex = LaunchExtras()) {
-  if (n_models == 0) return GRN_OK;
+// Chooses the plan of a launch of `n_models` packed records already on the
+// device (timing candidate plans on `stream` the first time a batch shape is
+// seen) and fills its arguments, state slots bound: everything but
+// enqueueing it.
+grn_status prepare_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
+                          int n_models, int max_genes, int max_links,
+                          const double *d_max_error, double *d_raw, int32_t *d_steps,
+                          int32_t *d_flag, cudaStream_t stream, LaunchPlan *plan_out,
+                          grn::SimArgs *args_out, const LaunchExtras &ex) {
   if (ctx->n_exp < 1) return fail(ctx, GRN_ERR_NO_EXPERIMENTS, "no experiments uploaded");
   const bool trace = ex.trace != nullptr;
   std::vector<std::pair<double, LaunchPlan>> plans;
@@ -446,9 +465,114 @@ grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_of
       ctx->tuned[key] = grn_ctx::Tuned{plan.v, plan.cluster, plan.planes, 0.0};
     }
   }
-  s = launch_plan(ctx, plan, a, stream);
+  s = bind_state(ctx, plan, &a);
+  if (s != GRN_OK) return s;
+  *plan_out = plan;
+  *args_out = a;
+  return GRN_OK;
+}
+
+// Launches the simulation of `n_models` packed records already on the
+// device.  `stream` may differ from the context's stream.
+grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_offsets,
+                         int n_models, int max_genes, int max_links,
+                         const double *d_max_error, double *d_raw, int32_t *d_steps,
+                         int32_t *d_flag, cudaStream_t stream, LaunchPlan *plan_out,
+                         const LaunchExtras &ex = LaunchExtras()) {
+  if (n_models == 0) return GRN_OK;
+  LaunchPlan plan;
+  grn::SimArgs a;
+  grn_status s = prepare_packed(ctx, d_words, d_offsets, n_models, max_genes, max_links,
+                                d_max_error, d_raw, d_steps, d_flag, stream, &plan, &a, ex);
+  if (s != GRN_OK) return s;
+  s = enqueue_plan(ctx, plan, a, stream);
   if (s != GRN_OK) return s;
   if (plan_out) *plan_out = plan;
+  return GRN_OK;
+}
+
+// The autotuner has not yet chosen a plan for this batch shape.
+bool tuning_needed(grn_ctx *ctx, int n_models, int max_genes, int max_links) {
+  if (ctx->forced_schedule != GRN_SCHEDULE_AUTO || !ctx->autotune) return false;
+  const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
+  const std::array<int, 7> key = {ctx->p.dim_x, ctx->p.dim_y, max_genes, max_links, ctx->n_exp,
+                                  ctx->fast_ok ? 1 : 0, bucket};
+  return ctx->tuned.find(key) == ctx->tuned.end();
+}
+
+void fill_launch_stats(grn_eval_stats *stats, int n, std::chrono::steady_clock::time_point t0,
+                       std::chrono::steady_clock::time_point t1, size_t h2d, size_t d2h,
+                       const LaunchPlan &plan) {
+  std::memset(stats, 0, sizeof *stats);
+  stats->n_models = n;
+  stats->pack_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  stats->h2d_bytes = (int64_t)h2d;
+  stats->d2h_bytes = (int64_t)d2h;
+  stats->schedule = plan.schedule;
+  stats->threads_per_block = plan.v.threads;
+  stats->blocks = plan.blocks;
+  stats->cluster_size = std::max(1, plan.cluster);
+}
+
+// Graph mode: the job's copy-in, kernel, copy-out and timing events as one
+// CUDA graph, captured from the stream and replayed.  A job keeps its
+// instantiated graph; the next capture only updates its parameters (sizes,
+// kernel arguments) when the plan keeps the graph's shape, else it is
+// instantiated again.  Plan selection (with any autotuning) stays outside
+// the capture.
+grn_status enqueue_job_graph(grn_ctx *ctx, Job *j, int n, const PackedHost &ph, size_t wb,
+                             size_t ob, size_t eb, size_t sb, LaunchPlan *plan_out) {
+  cudaStream_t st = ctx->stream;
+  LaunchPlan plan{};
+  grn::SimArgs a{};
+  grn_status s = prepare_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
+                                static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes,
+                                ph.max_links, static_cast<const double *>(j->d_maxerr.p),
+                                static_cast<double *>(j->d_raw.p),
+                                static_cast<int32_t *>(j->d_steps.p),
+                                static_cast<int32_t *>(j->d_flag.p), st, &plan, &a,
+                                LaunchExtras());
+  if (s != GRN_OK) return s;
+  GRN_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(cudaMemcpyAsync(j->d_words.p, j->h_words.p, wb, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j->d_offsets.p, j->h_offsets.p, ob, cudaMemcpyHostToDevice, st));
+  chk(cudaMemcpyAsync(j->d_maxerr.p, j->h_maxerr.p, eb, cudaMemcpyHostToDevice, st));
+  chk(cudaMemsetAsync(j->d_flag.p, 0, 4, st));
+  chk(cudaEventRecordWithFlags(j->ev_start, st, cudaEventRecordExternal));
+  if (e == cudaSuccess) s = enqueue_plan(ctx, plan, a, st);
+  chk(cudaEventRecordWithFlags(j->ev_kernel, st, cudaEventRecordExternal));
+  chk(cudaMemcpyAsync(j->h_raw.p, j->d_raw.p, eb, cudaMemcpyDeviceToHost, st));
+  chk(cudaMemcpyAsync(j->h_steps.p, j->d_steps.p, sb, cudaMemcpyDeviceToHost, st));
+  chk(cudaMemcpyAsync(j->h_flag.p, j->d_flag.p, 4, cudaMemcpyDeviceToHost, st));
+  chk(cudaEventRecordWithFlags(j->ev_done, st, cudaEventRecordExternal));
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+  if (s != GRN_OK || e != cudaSuccess || ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (s != GRN_OK) return s;
+    return cuda_fail(ctx, e != cudaSuccess ? e : ec, "graph capture");
+  }
+  bool updated = false;
+  if (j->exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(j->exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(j->exec);
+      j->exec = nullptr;
+    }
+  }
+  if (!updated) e = cudaGraphInstantiate(&j->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    j->exec = nullptr;
+    return cuda_fail(ctx, e, "cudaGraphInstantiate");
+  }
+  GRN_CUDA(ctx, cudaGraphLaunch(j->exec, st));
+  *plan_out = plan;
   return GRN_OK;
 }
 
@@ -488,6 +612,14 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   std::memcpy(j->h_offsets.p, ph.offsets.data(), ob);
   std::memcpy(j->h_maxerr.p, max_error, eb);
   cudaStream_t st = ctx->stream;
+  if (ctx->graphs && !tuning_needed(ctx, n, ph.max_genes, ph.max_links)) {
+    LaunchPlan plan{};
+    s = enqueue_job_graph(ctx, j, n, ph, wb, ob, eb, sb, &plan);
+    if (s != GRN_OK) return s;
+    j->cells = (int64_t)ctx->p.dim_x * ctx->p.dim_y;
+    if (stats) fill_launch_stats(stats, n, t0, t1, wb + ob + eb, eb + sb + 4, plan);
+    return GRN_OK;
+  }
   GRN_CUDA(ctx, cudaMemcpyAsync(j->d_words.p, j->h_words.p, wb, cudaMemcpyHostToDevice, st));
   GRN_CUDA(ctx, cudaMemcpyAsync(j->d_offsets.p, j->h_offsets.p, ob, cudaMemcpyHostToDevice, st));
   GRN_CUDA(ctx, cudaMemcpyAsync(j->d_maxerr.p, j->h_maxerr.p, eb, cudaMemcpyHostToDevice, st));
@@ -506,17 +638,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   GRN_CUDA(ctx, cudaMemcpyAsync(j->h_flag.p, j->d_flag.p, 4, cudaMemcpyDeviceToHost, st));
   GRN_CUDA(ctx, cudaEventRecord(j->ev_done, st));
   j->cells = (int64_t)ctx->p.dim_x * ctx->p.dim_y;
-  if (stats) {
-    std::memset(stats, 0, sizeof *stats);
-    stats->n_models = n;
-    stats->pack_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    stats->h2d_bytes = (int64_t)(wb + ob + eb);
-    stats->d2h_bytes = (int64_t)(eb + sb + 4);
-    stats->schedule = plan.schedule;
-    stats->threads_per_block = plan.v.threads;
-    stats->blocks = plan.blocks;
-    stats->cluster_size = std::max(1, plan.cluster);
-  }
+  if (stats) fill_launch_stats(stats, n, t0, t1, wb + ob + eb, eb + sb + 4, plan);
   return GRN_OK;
 }
 
@@ -627,6 +749,12 @@ grn_status grn_destroy(grn_ctx *ctx) {
     if (b->p) cudaFree(b->p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return GRN_OK;
+}
+
+grn_status grn_set_graphs(grn_ctx *ctx, int enable) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  ctx->graphs = enable != 0;
   return GRN_OK;
 }
 

@@ -208,6 +208,14 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size);
  * call clears the cache. */
 grn_status grn_set_autotune(grn_ctx *ctx, int enable);
 
+/* enable = 1: grn_evaluate, grn_evaluate_batch and grn_submit replay one
+ * CUDA graph per in-flight job -- copy-in, simulation kernel, copy-out and
+ * timing events -- re-captured each call and updated in place (parameters
+ * only) while the launch plan keeps its shape, so a generation's GPU work is
+ * one graph launch.  A batch shape the autotuner has not timed yet is run
+ * once without a graph.  Off by default. */
+grn_status grn_set_graphs(grn_ctx *ctx, int enable);
+
 /* ------------------------------------------------------------ experiments */
 
 /* Uploads the experiments once (the reference uploads them once per device,

@@ -290,6 +290,34 @@ def test_trace_stops_with_the_simulation():
     assert len(frames) == st["total_steps"] // 10 + 1 < 1000
 
 
+def test_graph_mode_matches_stream_launches():
+    """Graph mode (one captured graph per job, updated in place) gives the
+    same errors as plain stream launches, across batch sizes that change
+    the graph's copy sizes and kernel arguments, and through submit/wait."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=22, n_models=200, steps=60,
+                                              W=24, H=20)
+    subsets = [np.arange(200), np.arange(37), np.arange(5, 180), np.arange(200)]
+    me = np.linspace(0.01, 5.0, 200)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        want = [ev.evaluate_batch(batch.subset(ix), me[ix])[:2] for ix in subsets]
+        ev.set_graphs(True)
+        for ix, (we, wr) in zip(subsets, want):
+            err, raw, st = ev.evaluate_batch(batch.subset(ix), me[ix])
+            np.testing.assert_array_equal(raw, wr)
+            np.testing.assert_array_equal(err, we)
+            assert st["kernel_ms"] > 0
+        for t, ix in enumerate(subsets[:3]):
+            ev.submit(t, batch.subset(ix), me[ix])
+        got = {}
+        for _ in range(3):
+            t, err, raw = ev.wait_any()
+            got[t] = (err, raw)
+        for t in range(3):
+            np.testing.assert_array_equal(got[t][1], want[t][1])
+            np.testing.assert_array_equal(got[t][0], want[t][0])
+
+
 def test_early_exit_and_steps():
     """minConcChange stops simulations early; the non-convergence penalty
     uses the running change sum."""
