@@ -268,6 +268,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--schedule", default="auto",
+                    choices=["auto", "fixed_items", "walk_items", "global", "cluster"],
+                    help="force a kernel schedule instead of the autotuner's choice")
     ap.add_argument("--pipeline", action="store_true",
                     help="island workloads: two deme halves alternate on the GPU while the "
                          "host breeds the other (same populations)")
@@ -313,6 +316,8 @@ def main():
     n = batch.n_models
     ev = grn.Evaluator(params, device=local)
     ev.set_experiments(init, tgt)
+    if args.schedule != "auto":  # a fixed schedule: no autotuning launches (profiling)
+        ev.set_schedule({v: k for k, v in grn.SCHEDULE_NAMES.items()}[args.schedule])
     pk = ev.pack(batch)
     info = pk.info
     me = torch.full((n,), 1000.0, dtype=torch.float64, device="cuda")

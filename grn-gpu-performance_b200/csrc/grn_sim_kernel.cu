@@ -61,6 +61,40 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
+// ---- paired FP32 arithmetic (PTX ISA: add/mul/fma .rn.f32x2, sm_100+) ---
+// Two lanes per instruction, each rounded exactly like its scalar
+// counterpart, so results are bit-identical to fmaf / + / *.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4 &v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+
 // Shared-memory copy of one model record.
 struct ModelSmem {
   PackedHeader hdr;
@@ -200,6 +234,25 @@ __device__ __forceinline__ void regulation(const ModelSmem &M, const PackedGene 
 // fixed register indices and no per-link dispatch is needed.  The result is
 // the fast combine's: min over OR terms, then max with each AND term (terms
 // are never NaN for fast models, and min/max are order-free).
+// Fast-path combine of one link into 4 running exponents: the terms
+// a * lg2(x) + b for two cells per instruction, then min (OR) or max (AND).
+template <bool AND>
+__device__ __forceinline__ void comb4_fast(float4 &v, float2 ab, const float4 &x) {
+  const float2 t01 = fma2(f2(ab.x), lo2(x), f2(ab.y));
+  const float2 t23 = fma2(f2(ab.x), hi2(x), f2(ab.y));
+  if (AND) {
+    v.x = fmaxf(v.x, t01.x);
+    v.y = fmaxf(v.y, t01.y);
+    v.z = fmaxf(v.z, t23.x);
+    v.w = fmaxf(v.w, t23.y);
+  } else {
+    v.x = fminf(v.x, t01.x);
+    v.y = fminf(v.y, t01.y);
+    v.z = fminf(v.z, t23.x);
+    v.w = fminf(v.w, t23.y);
+  }
+}
+
 template <int NI, int GMAX>
 __device__ __forceinline__ void regulation_dense(const ModelSmem &M, const DenseSmem &D, int p,
                                                  const float4 (&lg)[NI][GMAX],
@@ -221,7 +274,7 @@ __device__ __forceinline__ void regulation_dense(const ModelSmem &M, const Dense
     if ((os >> k) & 1u) {
       const float2 ab = D.ab[p][k];
 #pragma unroll
-      for (int i = 0; i < NI; ++i) comb4<kOrFast>(v[i], ab.x, lg[i][k], ab.y);
+      for (int i = 0; i < NI; ++i) comb4_fast<false>(v[i], ab, lg[i][k]);
     }
   }
   if (g.n_or == 0) {
@@ -242,15 +295,17 @@ __device__ __forceinline__ void regulation_dense(const ModelSmem &M, const Dense
     if ((as >> k) & 1u) {
       const float2 ab = D.ab[p][k];
 #pragma unroll
-      for (int i = 0; i < NI; ++i) comb4<kAndFast>(v[i], ab.x, lg[i][k], ab.y);
+      for (int i = 0; i < NI; ++i) comb4_fast<true>(v[i], ab, lg[i][k]);
     }
   }
 #pragma unroll
   for (int i = 0; i < NI; ++i) {
-    h[i].x = rcp_approx(1.0f + ex2_approx(v[i].x));
-    h[i].y = rcp_approx(1.0f + ex2_approx(v[i].y));
-    h[i].z = rcp_approx(1.0f + ex2_approx(v[i].z));
-    h[i].w = rcp_approx(1.0f + ex2_approx(v[i].w));
+    const float2 e01 = add2(f2(1.0f), make_float2(ex2_approx(v[i].x), ex2_approx(v[i].y)));
+    const float2 e23 = add2(f2(1.0f), make_float2(ex2_approx(v[i].z), ex2_approx(v[i].w)));
+    h[i].x = rcp_approx(e01.x);
+    h[i].y = rcp_approx(e01.y);
+    h[i].z = rcp_approx(e23.x);
+    h[i].w = rcp_approx(e23.y);
   }
 }
 
@@ -388,6 +443,48 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
   else
     regulation_dense<NI, GMAX>(M, D, p, lg, h);
   const bool diffuses = gn.dif > 0.0f;  // uniform: the same gene for the whole block
+  if constexpr (!EXACT) {
+    // Fast path (update_cell<false>) on cell pairs: the same roundings,
+    // two cells per FP32 instruction.
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const float4 c = *reinterpret_cast<const float4 *>(cur + it[i].base);
+      float2 r01 = fma2(f2(-gn.deg), lo2(c), mul2(f2(gn.lim), lo2(h[i])));
+      float2 r23 = fma2(f2(-gn.deg), hi2(c), mul2(f2(gn.lim), hi2(h[i])));
+      if (diffuses) {
+        const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
+        const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
+        float lft = __shfl_up_sync(kFull, c.w, 1);
+        float rgt = __shfl_down_sync(kFull, c.x, 1);
+        if (it[i].lfix) lft = cur[it[i].base - 1];
+        if (it[i].rfix) rgt = cur[it[i].base + 4];
+        if (it[i].lzero) lft = 0.0f;
+        if (it[i].rzero) rgt = 0.0f;
+        // Reference order: x-1, x+1, y-1, y+1.
+        const float2 s01 = add2(add2(add2(make_float2(lft, c.x), make_float2(c.y, c.z)),
+                                     lo2(up)), lo2(dn));
+        const float2 s23 = add2(add2(add2(make_float2(c.y, c.z), make_float2(c.w, rgt)),
+                                     hi2(up)), hi2(dn));
+        r01 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.x, -it[i].tot.y), lo2(c), s01), r01);
+        r23 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.z, -it[i].tot.w), hi2(c), s23), r23);
+      }
+      const float2 n01 = fma2(f2(dt), r01, lo2(c));
+      const float2 n23 = fma2(f2(dt), r23, hi2(c));
+      nv[i] = make_float4(fmaxf(n01.x, 0.0f), fmaxf(n01.y, 0.0f), fmaxf(n23.x, 0.0f),
+                          fmaxf(n23.y, 0.0f));
+      float m = fmaxf(fabsf(r01.x), 0.0f);
+      float m1 = fabsf(r01.y), m2 = fabsf(r23.x), m3 = fabsf(r23.y);
+      if constexpr (RAGGED) {
+        // Cells past W are padding: kept at 0, never part of the max.
+        if (!it[i].v1) { nv[i].y = 0.0f; m1 = 0.0f; }
+        if (!it[i].v2) { nv[i].z = 0.0f; m2 = 0.0f; }
+        if (!it[i].v3) { nv[i].w = 0.0f; m3 = 0.0f; }
+      }
+      m = fmaxf(fmaxf(m, m1), fmaxf(m2, m3));
+      if (it[i].valid) mx = fmaxf(mx, m);
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < NI; ++i) {
     const float4 c = *reinterpret_cast<const float4 *>(cur + it[i].base);
@@ -477,7 +574,10 @@ __device__ __forceinline__ float *plane_of(const StatePtrs &sp, const Geom &g, i
 
 // New values of all genes of NI groups: shared-memory genes first, then
 // global-memory genes (two loops so that each uses its own load path).
-template <int NI, int GMAX, bool EXACT, bool RAGGED>
+// GMAX is the launch's gene capacity (the global slot layout); GS >= the
+// model's gene count bounds the regulator slots the step evaluates (the
+// unrolled slot loops cost GS steps per gene whatever the links).
+template <int NI, int GMAX, int GS, bool EXACT, bool RAGGED>
 __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &D,
                                            const StatePtrs &sp,
                                            const Geom &g, const Item (&it)[NI], int par,
@@ -491,9 +591,9 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   // lg2 of every regulator gene's current value.  The dense (fast) path
   // reads an entry only under its slot bit, so entries of genes no link
   // reads are left unset there; the exact path's slot switch needs them 0.
-  float4 lg[NI][GMAX];
+  float4 lg[NI][GS];
 #pragma unroll
-  for (int k = 0; k < GMAX; ++k) {
+  for (int k = 0; k < GS; ++k) {
     {
 #pragma unroll
       for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
@@ -513,8 +613,8 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   for (int p = 0; p < sp.n_sm; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GMAX, EXACT, RAGGED>(M, D, p, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc,
-                                         mx, nv);
+    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc,
+                                       mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(sm_nxt + p * g.PS + it[i].base) = nv[i];
@@ -522,12 +622,33 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   for (int p = sp.n_sm; p < G; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GMAX, EXACT, RAGGED>(M, D, p, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc,
-                                         mx, nv);
+    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc,
+                                       mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(gl_nxt + p * g.PS + it[i].base) = nv[i];
   }
+}
+
+// The fast path of one step, with the slot bound fitted to the model's gene
+// count (a uniform branch per model).
+template <int NI, int GMAX, bool RAGGED>
+__device__ __forceinline__ void group_step_fast(const ModelSmem &M, const DenseSmem &D,
+                                                const StatePtrs &sp, const Geom &g,
+                                                const Item (&it)[NI], int par, float dt,
+                                                float min_conc, float &mx) {
+  const int G = M.hdr.n_genes;
+  if (GMAX > 2 && G <= 2)
+    group_step<NI, GMAX, (GMAX < 2 ? GMAX : 2), false, RAGGED>(M, D, sp, g, it, par, dt,
+                                                               min_conc, mx);
+  else if (GMAX > 4 && G <= 4)
+    group_step<NI, GMAX, (GMAX < 4 ? GMAX : 4), false, RAGGED>(M, D, sp, g, it, par, dt,
+                                                               min_conc, mx);
+  else if (GMAX > 6 && G <= 6)
+    group_step<NI, GMAX, (GMAX < 6 ? GMAX : 6), false, RAGGED>(M, D, sp, g, it, par, dt,
+                                                               min_conc, mx);
+  else
+    group_step<NI, GMAX, GMAX, false, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
 }
 
 // Pushes the edge rows of the new buffer (`nxt`) of every gene into the
@@ -741,9 +862,10 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
           // All ITEMS groups of the thread at once (items past the grid are
           // clamped duplicates and store nothing).
           if (exact)
-            group_step<ITEMS, GMAX, true, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
+            group_step<ITEMS, GMAX, GMAX, true, RAGGED>(M, D, sp, g, items, par, dt, min_conc,
+                                                        mx);
           else
-            group_step<ITEMS, GMAX, false, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
+            group_step_fast<ITEMS, GMAX, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
         } else {
           int y = ty0, gx = gx0;
           for (int i = 0; i < n_iter; ++i) {
@@ -751,9 +873,9 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
             const bool valid = q < g.Q;
             const Item it[1] = {valid ? make_item(y, gx, true, lane, g) : item_at(q, lane, g)};
             if (exact)
-              group_step<1, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
+              group_step<1, GMAX, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
             else
-              group_step<1, GMAX, false, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
+              group_step_fast<1, GMAX, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
             y += dy;
             gx += dgx;
             if (gx >= g.Wg) {
