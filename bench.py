@@ -269,7 +269,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--schedule", default="auto",
-                    choices=["auto", "fixed_items", "walk_items", "global", "cluster"],
+                    choices=["auto", "fixed_items", "walk_items", "global", "cluster", "stream"],
                     help="force a kernel schedule instead of the autotuner's choice")
     ap.add_argument("--pipeline", action="store_true",
                     help="island workloads: two deme halves alternate on the GPU while the "

@@ -134,7 +134,7 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
   double best_score = -1;
   for (int i = 0; i < sim_variant_count(); ++i) {
     const KernelVariant v = sim_variant(i);
-    if (v.cluster || v.trace || v.gmax < gmax || v.ragged != ragged || (!v.loop && Q > v.threads * v.items))
+    if (v.cluster || v.trace || v.stream || v.gmax < gmax || v.ragged != ragged || (!v.loop && Q > v.threads * v.items))
       continue;
     const int planes = std::min(fit, 2 * gmax);
     const size_t smem = fixed + planes * plane_bytes;

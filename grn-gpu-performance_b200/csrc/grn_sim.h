@@ -47,6 +47,7 @@ struct SimArgs {
   float *trace_out;          // optional trace frames [caller index][n_exp]
                              // [trace_frames][state_planes][H][W]
   int32_t trace_frames;
+  int32_t band_rows;         // streaming schedule: rows per staged band
 };
 
 // One compiled kernel variant.
@@ -59,6 +60,7 @@ struct KernelVariant {
   bool cluster; // cluster-split: a cluster of CTAs per model, one band of
                 // rows each
   bool trace;   // writes trace frames (SimArgs::trace_out)
+  bool stream;  // streaming schedule (SimArgs::band_rows)
 };
 
 // Launch plan chosen by the host.
@@ -71,6 +73,7 @@ struct LaunchPlan {
   int blocks_per_sm;
   int64_t slot_floats;   // floats of one block's global state slot (0: none)
   int cluster;           // CTAs per cluster (1: one CTA per model)
+  int band_rows;         // streaming schedule: rows per staged band (else 0)
 };
 
 // Floats of one state plane of a W x H grid: rows padded to float4 groups,

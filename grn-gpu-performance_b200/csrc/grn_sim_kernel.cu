@@ -95,6 +95,59 @@ __device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x,
 __device__ __forceinline__ float2 hi2(const float4 &v) { return make_float2(v.z, v.w); }
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 
+// ---- bulk copies and mbarriers (PTX ISA; streaming schedule) -----------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// One bulk copy global -> this CTA's shared memory, completing on `bar`.
+// Both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Waits for the phase with `parity` to complete, giving up after a bounded
+// number of polls (each try_wait itself blocks for a while): false on a
+// time-out, which the caller reports instead of hanging.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (uint32_t i = 0; i < (1u << 24); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Orders this thread's generic-proxy accesses before later async-proxy
+// (bulk copy) accesses of the same memory.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Shared-memory copy of one model record.
 struct ModelSmem {
   PackedHeader hdr;
@@ -130,7 +183,9 @@ constexpr size_t kWorkOffset = kDredOffset + 32 * 8;     // int [2]
 // step parity) and per-CTA fitness sums double [kMaxCluster].
 constexpr size_t kCmaxOffset = kWorkOffset + 16;
 constexpr size_t kCsumOffset = kCmaxOffset + 2 * kMaxCluster * 4;
-constexpr size_t kStateOffset = (kCsumOffset + kMaxCluster * 8 + 127) & ~size_t(127);
+// Two mbarriers of the streaming schedule's copy stages.
+constexpr size_t kMbarOffset = (kCsumOffset + kMaxCluster * 8 + 15) & ~size_t(15);
+constexpr size_t kStateOffset = (kMbarOffset + 16 + 127) & ~size_t(127);
 
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
 
@@ -651,6 +706,139 @@ __device__ __forceinline__ void group_step_fast(const ModelSmem &M, const DenseS
     group_step<NI, GMAX, GMAX, false, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
 }
 
+// ---- streaming schedule -------------------------------------------------
+//
+// For grids whose planes do not fit shared memory: every plane lives in the
+// block's global slot and each step walks the grid in bands of R rows.  A
+// band's rows plus one halo row above and below, of every gene, arrive in a
+// shared-memory stage by bulk copies (the TMA engine's cp.async.bulk, one
+// per gene, completing on the stage's mbarrier) while the previous band is
+// computed from the other stage; new values go straight to the global slot.
+// The step's arithmetic is the other schedules' (gene_update), so states
+// are bit-identical.
+
+// New values of all genes of NI groups of one band (stage planes of
+// gb.PS floats), written to the global next-state planes.
+template <int NI, int GS, bool EXACT, bool RAGGED>
+__device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseSmem &D,
+                                                const float *stage, int G, const Geom &gb,
+                                                const Item (&it)[NI], float *gl_nxt, size_t gps,
+                                                float dt, float min_conc, float &mx) {
+  const uint32_t lg_mask = M.hdr.lg_mask;
+  float4 lg[NI][GS];
+#pragma unroll
+  for (int k = 0; k < GS; ++k) {
+    {
+#pragma unroll
+      for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
+    }
+    if (k < G && ((lg_mask >> k) & 1u)) {
+      const float *pl = stage + k * gb.PS;
+#pragma unroll
+      for (int i = 0; i < NI; ++i) {
+        const float4 c = *reinterpret_cast<const float4 *>(pl + it[i].base);
+        lg[i][k].x = lg2_approx(c.x);
+        lg[i][k].y = lg2_approx(c.y);
+        lg[i][k].z = lg2_approx(c.z);
+        lg[i][k].w = lg2_approx(c.w);
+      }
+    }
+  }
+  // stage row 0 is plane row gb.y0 (grid row gb.y0 - 1)
+  float *out = gl_nxt + (size_t)gb.y0 * gb.RS;
+  for (int p = 0; p < G; ++p) {
+    float4 nv[NI];
+    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, M.genes[p], lg, stage + p * gb.PS, gb, it, dt,
+                                       min_conc, mx, nv);
+#pragma unroll
+    for (int i = 0; i < NI; ++i)
+      if (it[i].valid) *reinterpret_cast<float4 *>(out + p * gps + it[i].base) = nv[i];
+  }
+}
+
+template <int NI, int GMAX, bool RAGGED>
+__device__ __forceinline__ void band_group_step_any(bool exact, const ModelSmem &M,
+                                                    const DenseSmem &D, const float *stage, int G,
+                                                    const Geom &gb, const Item (&it)[NI],
+                                                    float *gl_nxt, size_t gps, float dt,
+                                                    float min_conc, float &mx) {
+  if (exact)
+    band_group_step<NI, GMAX, true, RAGGED>(M, D, stage, G, gb, it, gl_nxt, gps, dt, min_conc,
+                                            mx);
+  else if (GMAX > 2 && G <= 2)
+    band_group_step<NI, (GMAX < 2 ? GMAX : 2), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+                                                              gps, dt, min_conc, mx);
+  else if (GMAX > 4 && G <= 4)
+    band_group_step<NI, (GMAX < 4 ? GMAX : 4), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+                                                              gps, dt, min_conc, mx);
+  else if (GMAX > 6 && G <= 6)
+    band_group_step<NI, (GMAX < 6 ? GMAX : 6), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+                                                              gps, dt, min_conc, mx);
+  else
+    band_group_step<NI, GMAX, false, RAGGED>(M, D, stage, G, gb, it, gl_nxt, gps, dt, min_conc,
+                                             mx);
+}
+
+// One Euler step of the streaming schedule.  Stages alternate by band; the
+// copy of band b + 2 is issued (thread 0) once every thread has finished
+// band b.  mphase holds each stage's next wait parity across steps.
+// Returns false (the same in every thread) if a copy did not complete in
+// time; the copies still in flight have then been waited for (bounded).
+template <int NT, int GMAX, bool RAGGED>
+__device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSmem &D,
+                            const StatePtrs &sp, const Geom &g, int G, int par, bool exact,
+                            float dt, float min_conc, float &mx, uint64_t *bars,
+                            uint32_t &mphase, int lane) {
+  const int R = A.band_rows;
+  const int nb = (g.H + R - 1) / R;
+  const int SPS = (R + 2) * g.RS;
+  float *stage0 = sp.sm;
+  const size_t gps = (size_t)g.PS;
+  const float *gl_cur = sp.gl + (par ? GMAX : 0) * gps;
+  float *gl_nxt = sp.gl + (par ? 0 : GMAX) * gps;
+  auto issue = [&](int b) {
+    float *st = stage0 + (b & 1) * GMAX * SPS;
+    const int rows = min(R + 2, g.H + 2 - b * R);  // plane rows b*R .. b*R + rows - 1
+    const uint32_t bytes = (uint32_t)rows * g.RS * 4u;
+    fence_proxy_async_shared();
+    mbar_expect_tx(bars + (b & 1), bytes * (uint32_t)G);
+    for (int p = 0; p < G; ++p)
+      bulk_g2s(st + p * SPS, gl_cur + p * gps + (size_t)b * R * g.RS, bytes, bars + (b & 1));
+  };
+  if (threadIdx.x == 0) {
+    issue(0);
+    if (nb > 1) issue(1);
+  }
+  for (int b = 0; b < nb; ++b) {
+    const int s = b & 1;
+    const uint32_t parity = (mphase >> s) & 1u;
+    const bool ok = mbar_wait(bars + s, parity);
+    mphase ^= 1u << s;
+    if (!__syncthreads_and(ok)) {
+      // Bounded second waits: the timed-out copy and the one issued ahead.
+      mbar_wait(bars + s, parity);
+      if (b + 1 < nb) mbar_wait(bars + (s ^ 1), (mphase >> (s ^ 1)) & 1u);
+      return false;
+    }
+    Geom gb = g;
+    gb.y0 = b * R;
+    gb.H = min(R, g.H - b * R);
+    gb.PS = SPS;
+    gb.Q = gb.H * g.Wg;
+    const float *st = stage0 + s * GMAX * SPS;
+    const int n_it = (gb.Q + NT - 1) / NT;
+    for (int i = 0; i < n_it; ++i) {  // every lane of a warp iterates together (shuffles)
+      const Item it[1] = {item_at(threadIdx.x + i * NT, lane, gb)};
+      band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st, G, gb, it, gl_nxt, gps, dt,
+                                            min_conc, mx);
+    }
+    __syncthreads();  // stage s is free again
+    if (threadIdx.x == 0 && b + 2 < nb) issue(b + 2);
+  }
+  fence_proxy_async_global();  // this step's writes before the next step's copies
+  return true;
+}
+
 // Pushes the edge rows of the new buffer (`nxt`) of every gene into the
 // neighbouring bands' halo rows: the first row to the band above (its row
 // Hb + 1), the last row to the band below (its row 0).  Shared-memory planes
@@ -710,13 +898,15 @@ __device__ __forceinline__ void cluster_share(T *slots, T v, int rank, int C) {
 //   RAGGED  W is not a multiple of 4
 //   TRACE   writes trace frames (trace_out) during the step loop; only the
 //           variants compiled for it carry that code
+//   ST      streaming schedule: planes in the global slot, bands of
+//           A.band_rows rows staged through shared memory by bulk copies
 //   CL      cluster-split: a cluster of C CTAs (launch attribute) simulates
 //           one model at a time, CTA r owning rows [r*Hb, r*Hb + Hb) with
 //           Hb = ceil(H / C).  Every CTA of a cluster takes the same branches
 //           and passes the same cluster barriers: the model index, the step
 //           max and the fitness sum are shared values, identical bits in
 //           every CTA.
-template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL, bool TRACE>
+template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL, bool TRACE, bool ST>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
@@ -750,16 +940,27 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   sp.sm = reinterpret_cast<float *>(smem + kStateOffset);
   sp.gl = A.gstate ? A.gstate + (size_t)blockIdx.x * (size_t)A.slot_floats : nullptr;
 
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kMbarOffset);
+  uint32_t mphase = 0;  // streaming: next wait parity of each stage
+  if constexpr (ST) {
+    if (tid == 0) {
+      mbar_init(bars, 1);
+      mbar_init(bars + 1, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+
   // Fixed items: geometry once per launch.
   Item items[LOOP ? 1 : ITEMS];
   if constexpr (!LOOP) {
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) items[i] = item_at(tid + i * NT, lane, g);
   }
-  // Walking items: start and per-iteration stride of (row, group column).
-  const int ty0 = tid / g.Wg, gx0 = tid - ty0 * g.Wg;
-  const int dy = NT / g.Wg, dgx = NT - dy * g.Wg;
-  const int n_iter = (g.Q + NT - 1) / NT;
+  // Walking items: per-iteration stride (ITEMS * NT groups) in (row, group
+  // column).
+  const int dy = (ITEMS * NT) / g.Wg, dgx = ITEMS * NT - dy * g.Wg;
+  const int n_iter = (g.Q + ITEMS * NT - 1) / (ITEMS * NT);
   // Items per thread of a full band: the same in every CTA of a cluster.
   const int n_iter_band = (Hb * g.Wg + NT - 1) / NT;
 
@@ -802,7 +1003,8 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
     const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast));
     const bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
                      M.hdr.n_links > GRN_MAX_LINKS || (sp.n_sm < G && sp.gl == nullptr) ||
-                     (!LOOP && n_iter_band > ITEMS);
+                     (!LOOP && n_iter_band > ITEMS) ||
+                     (ST && (A.band_rows < 1 || sp.gl == nullptr || A.planes != 0));
     if (bad) {
       if (tid == 0 && rank == 0) {
         atomicExch(A.error_flag, 1);
@@ -840,6 +1042,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         float *pl = plane_of<GMAX>(sp, g, kk, kb < G ? 0 : 1);
         pl[r] = v;
       }
+      if constexpr (ST) fence_proxy_async_global();  // before the first bulk copies
       if constexpr (CL) cg::this_cluster().sync();
       else __syncthreads();
 
@@ -858,7 +1061,16 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       int par = 0;  // buffer holding the current values
       while (step < A.n_steps && change > A.min_conc_change) {
         float mx = 0.0f;
-        if constexpr (!LOOP) {
+        if constexpr (ST) {
+          if (!stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
+                                              bars, mphase, lane)) {
+            if (tid == 0) {
+              atomicExch(A.error_flag, 2);
+              A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
+            }
+            return;  // every thread of the block: the decision is block-uniform
+          }
+        } else if constexpr (!LOOP) {
           // All ITEMS groups of the thread at once (items past the grid are
           // clamped duplicates and store nothing).
           if (exact)
@@ -867,20 +1079,34 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
           else
             group_step_fast<ITEMS, GMAX, RAGGED>(M, D, sp, g, items, par, dt, min_conc, mx);
         } else {
-          int y = ty0, gx = gx0;
+          // ITEMS groups per iteration (more loads in flight), each
+          // advanced by ITEMS * NT groups.
+          int y[ITEMS], gx[ITEMS];
+#pragma unroll
+          for (int j = 0; j < ITEMS; ++j) {
+            y[j] = (tid + j * NT) / g.Wg;
+            gx[j] = (tid + j * NT) - y[j] * g.Wg;
+          }
           for (int i = 0; i < n_iter; ++i) {
-            const int q = tid + i * NT;
-            const bool valid = q < g.Q;
-            const Item it[1] = {valid ? make_item(y, gx, true, lane, g) : item_at(q, lane, g)};
+            Item it[ITEMS];
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+              const int q = tid + (i * ITEMS + j) * NT;
+              it[j] = q < g.Q ? make_item(y[j], gx[j], true, lane, g) : item_at(q, lane, g);
+            }
             if (exact)
-              group_step<1, GMAX, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
+              group_step<ITEMS, GMAX, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc,
+                                                          mx);
             else
-              group_step_fast<1, GMAX, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
-            y += dy;
-            gx += dgx;
-            if (gx >= g.Wg) {
-              gx -= g.Wg;
-              ++y;
+              group_step_fast<ITEMS, GMAX, RAGGED>(M, D, sp, g, it, par, dt, min_conc, mx);
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+              y[j] += dy;
+              gx[j] += dgx;
+              if (gx[j] >= g.Wg) {
+                gx[j] -= g.Wg;
+                ++y[j];
+              }
             }
           }
         }
@@ -956,9 +1182,12 @@ struct VariantEntry {
   KernelFn fn;
 };
 
-#define GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, TR)                                      \
-  {{NT, GMAX, ITEMS, LOOP, false, CL, TR}, &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL, TR>}, \
-  {{NT, GMAX, ITEMS, LOOP, true, CL, TR}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL, TR>}
+#define GRN_VARIANT_X(NT, GMAX, ITEMS, LOOP, CL, TR, ST)                                   \
+  {{NT, GMAX, ITEMS, LOOP, false, CL, TR, ST},                                            \
+   &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL, TR, ST>},                                \
+  {{NT, GMAX, ITEMS, LOOP, true, CL, TR, ST}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL, TR, ST>}
+#define GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, TR) \
+  GRN_VARIANT_X(NT, GMAX, ITEMS, LOOP, CL, TR, false)
 #define GRN_VARIANT(NT, GMAX, ITEMS, LOOP, CL) GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, false)
 
 const VariantEntry kVariants[] = {
@@ -972,6 +1201,9 @@ const VariantEntry kVariants[] = {
     GRN_VARIANT(512, 8, 1, true, true),    GRN_VARIANT(512, 16, 1, true, true),
     // trace frames (one model at a time: any grid, any gene count)
     GRN_VARIANT_T(256, 16, 1, true, false, true),
+    // streaming (bands staged by bulk copies)
+    GRN_VARIANT_X(512, 8, 1, true, false, false, true),
+    GRN_VARIANT_X(512, 16, 1, true, false, false, true),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -980,7 +1212,7 @@ const VariantEntry *find_variant(const KernelVariant &v) {
     const KernelVariant &k = kVariants[i].v;
     if (k.threads == v.threads && k.gmax == v.gmax && k.items == v.items &&
         k.loop == v.loop && k.ragged == v.ragged && k.cluster == v.cluster &&
-        k.trace == v.trace)
+        k.trace == v.trace && k.stream == v.stream)
       return &kVariants[i];
   }
   return nullptr;

@@ -30,7 +30,9 @@ FITNESS_REF_LOGTHRESH = 0
 FITNESS_MSE = 1
 SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1, 2, 3
 SCHEDULE_CLUSTER = 4
-SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster"}
+SCHEDULE_STREAM = 5
+SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster",
+                  5: "stream"}
 
 
 class SimParams(ctypes.Structure):

@@ -196,6 +196,21 @@ int host_threads() {
 // all-shared-memory state over state spilling to global slots.
 // Every feasible launch plan for a batch, with the heuristic throughput
 // score of each.
+// Rows per staged band of the streaming schedule: two stages of
+// gmax x (rows + 2) padded rows must fit the shared memory left over, one
+// stage's bytes must stay below the mbarrier transaction limit (2^20), and
+// a multiple of NT / Wg rows keeps every thread busy when Wg divides NT.
+int stream_rows(int W, int H, int gmax, size_t room, int threads) {
+  const int Wg = (W + 3) / 4;
+  const size_t row_bytes = (size_t)4 * Wg * sizeof(float);
+  long r = (long)(room / (2 * gmax * row_bytes)) - 2;
+  r = std::min<long>(r, H);
+  while (r > 1 && (size_t)gmax * (r + 2) * row_bytes >= (size_t)1 << 20) --r;
+  if (r < 1) return 0;
+  if (threads % Wg == 0 && r >= threads / Wg) r -= r % (threads / Wg);
+  return (int)r;
+}
+
 grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace,
                            std::vector<std::pair<double, LaunchPlan>> *out) {
   const int W = ctx->p.dim_x, H = ctx->p.dim_y;
@@ -212,6 +227,34 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace
     const grn::KernelVariant v = grn::sim_variant(i);
     if (v.gmax < max_genes || v.ragged != ragged || v.trace != trace) continue;
     if (ctx->forced_threads && !trace && v.threads != ctx->forced_threads) continue;
+    if (v.stream) {
+      // Streaming: only where the planes do not all fit shared memory.
+      if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_STREAM) continue;
+      const size_t plane_bytes = (size_t)grn::plane_floats(W, H) * sizeof(float);
+      const int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) & ~1 : 0;
+      if (sched == GRN_SCHEDULE_AUTO && fit / 2 >= max_genes) continue;
+      const int R = stream_rows(W, H, v.gmax, optin > fixed ? optin - fixed : 0, v.threads);
+      if (R < 1) continue;
+      const size_t smem = fixed + (size_t)2 * v.gmax * (R + 2) * 4 * Wg * sizeof(float);
+      int per_sm = 0;
+      GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &per_sm));
+      const int ctas = per_sm * ctx->n_sm;
+      if (ctas < 1) continue;
+      LaunchPlan plan{};
+      plan.v = v;
+      plan.schedule = GRN_SCHEDULE_STREAM;
+      plan.planes = 0;
+      plan.smem_bytes = smem;
+      plan.blocks_per_sm = per_sm;
+      plan.slot_floats = 2LL * v.gmax * grn::plane_floats(W, H);
+      plan.cluster = 1;
+      plan.band_rows = R;
+      plan.blocks = std::max(1, std::min(n_models, ctas));
+      const double busy = (double)std::min(ctas, n_models) * std::min(v.threads, R * Wg);
+      out->push_back({busy * 0.9 - 1e-3 * v.gmax, plan});
+      continue;
+    }
+    if (sched == GRN_SCHEDULE_STREAM) continue;
     if (sched == GRN_SCHEDULE_CLUSTER && !v.cluster) continue;
     if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_CLUSTER && v.cluster) continue;
     if (sched == GRN_SCHEDULE_FIXED_ITEMS && v.loop) continue;
@@ -296,6 +339,7 @@ grn_status choose_plan(grn_ctx *ctx, int max_genes, int n_models, LaunchPlan *ou
 bool same_plan(const LaunchPlan &a, const grn::KernelVariant &v, int cluster, int planes) {
   return a.v.threads == v.threads && a.v.gmax == v.gmax && a.v.items == v.items &&
          a.v.loop == v.loop && a.v.ragged == v.ragged && a.v.cluster == v.cluster &&
+         a.v.stream == v.stream &&
          a.cluster == cluster && a.planes == planes;
 }
 
@@ -305,6 +349,7 @@ bool same_plan(const LaunchPlan &a, const grn::KernelVariant &v, int cluster, in
 // the slots if they grew).
 grn_status bind_state(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs *a) {
   a->planes = plan.planes;
+  a->band_rows = plan.band_rows;
   a->gstate = nullptr;
   a->slot_floats = 0;
   if (plan.slot_floats > 0) {
@@ -785,7 +830,7 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size) {
 
 grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block) {
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
-  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_CLUSTER || threads_per_block < 0)
+  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_STREAM || threads_per_block < 0)
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad schedule");
   ctx->forced_schedule = schedule;
   ctx->forced_threads = threads_per_block;

@@ -161,10 +161,14 @@ typedef enum grn_schedule {
                                    grid size                              */
   GRN_SCHEDULE_GLOBAL = 3,      /* walking groups, every plane in global
                                    memory                                 */
-  GRN_SCHEDULE_CLUSTER = 4      /* cluster-split: a thread-block cluster
+  GRN_SCHEDULE_CLUSTER = 4,     /* cluster-split: a thread-block cluster
                                    per model, each CTA a band of rows in
                                    its shared memory, halo rows exchanged
                                    through distributed shared memory      */
+  GRN_SCHEDULE_STREAM = 5       /* every plane in global memory; each step
+                                   walks bands of rows staged through
+                                   shared memory by bulk (TMA) copies,
+                                   double-buffered                        */
 } grn_schedule;
 
 typedef struct grn_ctx grn_ctx;

@@ -255,6 +255,29 @@ def test_autotuned_plan_is_cached_and_exact():
     assert_raw_close(a_raw, h_raw, rtol=1e-12, atol=0, what="autotune")
 
 
+@pytest.mark.parametrize("W,H,steps,genes", [(256, 256, 12, (8, 8)), (100, 100, 30, (6, 8)),
+                                             (30, 37, 25, (2, 8)), (250, 90, 15, (8, 16))])
+def test_stream_schedule_matches_global_bitwise(W, H, steps, genes):
+    """Bands staged through shared memory by bulk copies (streaming
+    schedule): the same per-cell arithmetic as the all-global schedule,
+    identical states, including ragged widths, a last band shorter than the
+    others, 16-gene models and the exact path (links with K = 0)."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=23, n_models=12, steps=steps,
+                                              W=W, H=H, genes=genes, links=(1, 24), n_exp=2)
+    batch.links["dis_const"][0] = 0.0  # model 0 takes the exact path
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=16)
+        ev.set_schedule(grn.SCHEDULE_STREAM)
+        raw, states = ev.evaluate_states(batch, max_planes=16)
+        _, raw_b, st = ev.evaluate_batch(batch)
+    assert st["schedule"] == grn.SCHEDULE_STREAM
+    assert np.array_equal(states, base_states)
+    assert np.array_equal(raw, raw_b)
+    assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream")
+
+
 def test_cluster_schedule_rejects_empty_bands():
     params, batch, init, tgt = synth.workload("small_32x32", seed=17, n_models=4, steps=10,
                                               W=32, H=20)
