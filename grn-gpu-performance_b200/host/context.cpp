@@ -251,7 +251,9 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace
       plan.band_rows = R;
       plan.blocks = std::max(1, std::min(n_models, ctas));
       const double busy = (double)std::min(ctas, n_models) * std::min(v.threads, R * Wg);
-      out->push_back({busy * 0.9 - 1e-3 * v.gmax, plan});
+      // Heuristic rank below the walking / all-global plans (faster only where the
+      // slots' traffic leaves L2); the autotuner measures it against them.
+      out->push_back({busy * 0.6 - 1e-3 * v.gmax, plan});
       continue;
     }
     if (sched == GRN_SCHEDULE_STREAM) continue;
