@@ -48,7 +48,11 @@ struct SimArgs {
                              // [trace_frames][state_planes][H][W]
   int32_t trace_frames;
   int32_t band_rows;         // streaming schedule: rows per staged band
+  int32_t test_hooks;        // kHook* bits (tests of the error paths)
 };
+
+// Test hooks (grn_set_test_hooks): make a bounded wait run out on purpose.
+constexpr int32_t kHookWithholdBandCopy = 1;  // streaming: band 1's copy is never issued
 
 // One compiled kernel variant.
 struct KernelVariant {

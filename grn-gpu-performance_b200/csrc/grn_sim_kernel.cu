@@ -131,12 +131,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Waits for the phase with `parity` to complete, giving up after a bounded
-// number of polls (each try_wait itself blocks for a while): false on a
-// time-out, which the caller reports instead of hanging.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase with `parity` to complete, giving up after about one
+// second (a bulk copy of a band takes microseconds): false on a time-out,
+// which the caller reports through the error flag instead of hanging.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t i = 0; i < (1u << 24); ++i)
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 0; i < (1u << 30); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > 1000000000ull) return false;
+  }
   return false;
 }
 // Orders this thread's generic-proxy accesses before later async-proxy
@@ -805,9 +814,11 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     for (int p = 0; p < G; ++p)
       bulk_g2s(st + p * SPS, gl_cur + p * gps + (size_t)b * R * g.RS, bytes, bars + (b & 1));
   };
+  // Test hook: withhold band 1's copy, so that its wait runs out.
+  const bool withhold = A.test_hooks & kHookWithholdBandCopy;
   if (threadIdx.x == 0) {
     issue(0);
-    if (nb > 1) issue(1);
+    if (nb > 1 && !withhold) issue(1);
   }
   for (int b = 0; b < nb; ++b) {
     const int s = b & 1;
@@ -815,8 +826,9 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     const bool ok = mbar_wait(bars + s, parity);
     mphase ^= 1u << s;
     if (!__syncthreads_and(ok)) {
-      // Bounded second waits: the timed-out copy and the one issued ahead.
-      mbar_wait(bars + s, parity);
+      // Bounded second waits for copies that may still be in flight: the
+      // timed-out one (unless withheld) and the one issued ahead.
+      if (!withhold) mbar_wait(bars + s, parity);
       if (b + 1 < nb) mbar_wait(bars + (s ^ 1), (mphase >> (s ^ 1)) & 1u);
       return false;
     }

@@ -31,6 +31,7 @@ FITNESS_MSE = 1
 SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1, 2, 3
 SCHEDULE_CLUSTER = 4
 SCHEDULE_STREAM = 5
+TEST_WITHHOLD_BAND_COPY = 1
 SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster",
                   5: "stream"}
 
@@ -117,6 +118,7 @@ _SIGNATURES = {
     "grn_set_cluster_size": ([_P, _I], _I),
     "grn_set_autotune": ([_P, _I], _I),
     "grn_set_graphs": ([_P, _I], _I),
+    "grn_set_test_hooks": ([_P, _I], _I),
     "grn_set_experiments": ([_P, _I, _P, _P], _I),
     "grn_set_experiments_rgb": ([_P, _I, _P, _P], _I),
     "grn_decode_rgb": ([_I, _I, _I, _P, _P], _I),
@@ -327,6 +329,9 @@ class Evaluator:
     def set_schedule(self, schedule, threads=0, cluster_size=0):
         _check(self.lib.grn_set_schedule(self.ctx, schedule, threads), self.ctx)
         _check(self.lib.grn_set_cluster_size(self.ctx, cluster_size), self.ctx)
+
+    def set_test_hooks(self, hooks):
+        _check(self.lib.grn_set_test_hooks(self.ctx, int(hooks)), self.ctx)
 
     def set_graphs(self, enable=True):
         _check(self.lib.grn_set_graphs(self.ctx, int(bool(enable))), self.ctx)

@@ -74,6 +74,7 @@ struct grn_ctx {
   int forced_schedule = GRN_SCHEDULE_AUTO;
   int forced_threads = 0;
   int forced_cluster = 0;
+  int test_hooks = 0;   // grn_set_test_hooks
   bool graphs = false;  // evaluations replay one CUDA graph per job
   // Measured autotuning of GRN_SCHEDULE_AUTO: the fastest plan timed on a
   // sample of the first batch of each shape, by (W, H, max genes, max links,
@@ -103,6 +104,14 @@ namespace {
 grn_status fail(grn_ctx *ctx, grn_status s, const std::string &msg) {
   if (ctx) ctx->last_error = msg;
   return s;
+}
+
+// The kernel's error flag: 1 a model record it cannot run, 2 a bounded
+// wait for a bulk copy that ran out (streaming schedule).
+grn_status kernel_flag_error(grn_ctx *ctx, int32_t flag) {
+  return fail(ctx, GRN_ERR_KERNEL,
+              flag == 2 ? "the simulation kernel's wait for a bulk copy timed out"
+                        : "the simulation kernel rejected a model record");
 }
 
 grn_status cuda_fail(grn_ctx *ctx, cudaError_t e, const char *what) {
@@ -495,6 +504,7 @@ grn_status prepare_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_o
   a.trace_every = ex.trace_every;
   a.trace_frames = ex.trace_frames;
   a.fast_ok = ctx->fast_ok ? 1 : 0;
+  a.test_hooks = ctx->test_hooks;
   if (ex.experiment >= 0) {
     const size_t cells = (size_t)W * H;
     a.initial += (size_t)ex.experiment * a.n_in * cells;
@@ -705,7 +715,7 @@ grn_status finish_job(grn_ctx *ctx, Job *j, const double *max_error, double *err
   const int n = j->n_models;
   if (n == 0) return GRN_OK;
   if (*static_cast<int32_t *>(j->h_flag.p) != 0)
-    return fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected a model record");
+    return kernel_flag_error(ctx, *static_cast<int32_t *>(j->h_flag.p));
   const double *raw = static_cast<const double *>(j->h_raw.p);
   const int32_t *steps = static_cast<const int32_t *>(j->h_steps.p);
   int64_t total_steps = 0;
@@ -805,6 +815,14 @@ grn_status grn_destroy(grn_ctx *ctx) {
     if (b->p) cudaFree(b->p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return GRN_OK;
+}
+
+static_assert(grn::kHookWithholdBandCopy == GRN_TEST_WITHHOLD_BAND_COPY, "test hook bits");
+
+grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks) {
+  if (!ctx || (hooks & ~GRN_TEST_WITHHOLD_BAND_COPY)) return GRN_ERR_INVALID_ARGUMENT;
+  ctx->test_hooks = hooks;
   return GRN_OK;
 }
 
@@ -967,7 +985,7 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
     chk(cudaMemcpyAsync(&flag, j.d_flag.p, 4, cudaMemcpyDeviceToHost, st));
     chk(cudaStreamSynchronize(st));
     if (s == GRN_OK && e == cudaSuccess && flag)
-      s = fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected a model record");
+      s = kernel_flag_error(ctx, flag);
   }
   cudaFree(d_states.p);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "grn_evaluate_states");
@@ -1172,7 +1190,7 @@ grn_status grn_trace_model(grn_ctx *ctx, const grn_product *products, int n_prod
   cudaFree(d_trace.p);
   if (s != GRN_OK) return s;
   if (e != cudaSuccess) return cuda_fail(ctx, e, "trace");
-  if (flag) return fail(ctx, GRN_ERR_KERNEL, "the simulation kernel rejected the model");
+  if (flag) return kernel_flag_error(ctx, flag);
   *n_frames = std::min(max_frames, steps / every + 1);
   if (labels_out) {
     const std::vector<int> labels = grn::labels_in_use(links, n_links, n_morph);

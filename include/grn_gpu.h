@@ -221,6 +221,14 @@ grn_status grn_set_autotune(grn_ctx *ctx, int enable);
  * once without a graph.  Off by default. */
 grn_status grn_set_graphs(grn_ctx *ctx, int enable);
 
+/* Tests of the error paths only.  GRN_TEST_WITHHOLD_BAND_COPY: the
+ * streaming schedule never issues the bulk copy of each step's second band,
+ * so the kernel's bounded wait for it runs out (about one second per model),
+ * the model's raw error becomes NaN and the call returns GRN_ERR_KERNEL; the
+ * context stays usable.  0 restores normal operation. */
+#define GRN_TEST_WITHHOLD_BAND_COPY 1
+grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks);
+
 /* ------------------------------------------------------------ experiments */
 
 /* Uploads the experiments once (the reference uploads them once per device,

@@ -278,6 +278,29 @@ def test_stream_schedule_matches_global_bitwise(W, H, steps, genes):
     assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream")
 
 
+def test_stream_copy_wait_times_out_cleanly():
+    """A bulk copy that never arrives (test hook): the kernel's bounded wait
+    runs out after about a second, the call reports it, and the context
+    keeps working."""
+    import time
+    params, batch, init, tgt = synth.workload("large_256x256", seed=24, n_models=2, steps=5)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_STREAM)
+        ev.set_test_hooks(grn.TEST_WITHHOLD_BAND_COPY)
+        t0 = time.perf_counter()
+        with pytest.raises(grn.GrnError) as e:
+            ev.evaluate_batch(batch)
+        assert "timed out" in str(e.value)
+        assert time.perf_counter() - t0 < 30
+        ev.set_test_hooks(0)
+        _, raw, _ = ev.evaluate_batch(batch)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        _, want, _ = ev.evaluate_batch(batch)
+    assert np.isfinite(raw).all()
+    np.testing.assert_array_equal(raw, want)
+
+
 def test_cluster_schedule_rejects_empty_bands():
     params, batch, init, tgt = synth.workload("small_32x32", seed=17, n_models=4, steps=10,
                                               W=32, H=20)
