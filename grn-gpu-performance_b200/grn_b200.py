@@ -117,6 +117,7 @@ _SIGNATURES = {
     "grn_set_schedule": ([_P, _I, _I], _I),
     "grn_set_cluster_size": ([_P, _I], _I),
     "grn_set_autotune": ([_P, _I], _I),
+    "grn_autotune_report": ([_P, _P, _I], _I),
     "grn_set_graphs": ([_P, _I], _I),
     "grn_set_test_hooks": ([_P, _I], _I),
     "grn_set_experiments": ([_P, _I, _P, _P], _I),
@@ -335,6 +336,11 @@ class Evaluator:
 
     def set_graphs(self, enable=True):
         _check(self.lib.grn_set_graphs(self.ctx, int(bool(enable))), self.ctx)
+
+    def autotune_report(self):
+        buf = ctypes.create_string_buffer(8192)
+        self.lib.grn_autotune_report(self.ctx, buf, len(buf))
+        return buf.value.decode()
 
     def set_autotune(self, enable=True):
         _check(self.lib.grn_set_autotune(self.ctx, int(bool(enable))), self.ctx)

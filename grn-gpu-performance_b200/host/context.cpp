@@ -86,6 +86,7 @@ struct grn_ctx {
     double ms;
   };
   std::map<std::array<int, 7>, Tuned> tuned;
+  std::string last_tuning;  // the last autotuning's candidates and times
   // minConc is 0 and the uploaded initial states are finite and
   // non-negative: the kernel's fast path then gives the same results as the
   // exact one (see the kernel's update_cell).
@@ -444,6 +445,18 @@ grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, Launc
   for (int i = 1; i < n_try; ++i)
     if (best_ms[i] < best_ms[best]) best = i;
   if (best != 0 && best_ms[best] > 0.97 * best_ms[0]) best = 0;
+  std::string rep;
+  for (int i = 0; i < n_try; ++i) {
+    const LaunchPlan &p = cand[i];
+    char line[200];
+    std::snprintf(line, sizeof line,
+                  "%s schedule %d threads %d gmax %d items %d cluster %d planes %d band %d "
+                  "ms %.4f\n",
+                  i == best ? "*" : " ", p.schedule, p.v.threads, p.v.gmax, p.v.items,
+                  std::max(1, p.cluster), p.planes, p.band_rows, best_ms[i]);
+    rep += line;
+  }
+  ctx->last_tuning = rep;
   if (best_ms[best] >= 1e30) return fail(ctx, GRN_ERR_CUDA, "autotune timed no plan");
   *out = plans[best].second;
   return GRN_OK;
@@ -819,6 +832,12 @@ grn_status grn_destroy(grn_ctx *ctx) {
 }
 
 static_assert(grn::kHookWithholdBandCopy == GRN_TEST_WITHHOLD_BAND_COPY, "test hook bits");
+
+grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len) {
+  if (!ctx || !buf || buf_len < 1) return GRN_ERR_INVALID_ARGUMENT;
+  std::snprintf(buf, (size_t)buf_len, "%s", ctx->last_tuning.c_str());
+  return (int)ctx->last_tuning.size() < buf_len ? GRN_OK : GRN_ERR_CAPACITY;
+}
 
 grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks) {
   if (!ctx || (hooks & ~GRN_TEST_WITHHOLD_BAND_COPY)) return GRN_ERR_INVALID_ARGUMENT;

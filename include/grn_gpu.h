@@ -213,6 +213,13 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size);
  * call clears the cache. */
 grn_status grn_set_autotune(grn_ctx *ctx, int enable);
 
+/* The last measured autotuning on this context, one line per timed plan
+ * ("*" marks the one kept): schedule, threads, gene capacity, items per
+ * thread, cluster size, shared-memory planes, streaming band rows and the
+ * fastest sample launch in ms.  GRN_ERR_CAPACITY if it was truncated to
+ * buf_len. */
+grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len);
+
 /* enable = 1: grn_evaluate, grn_evaluate_batch and grn_submit replay one
  * CUDA graph per in-flight job -- copy-in, simulation kernel, copy-out and
  * timing events -- re-captured each call and updated in place (parameters

@@ -278,6 +278,26 @@ def test_stream_schedule_matches_global_bitwise(W, H, steps, genes):
     assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream")
 
 
+def test_stream_schedule_early_exit_bitwise():
+    """Early exit under the streaming schedule: final states and step counts
+    match the all-global schedule."""
+    params, batch, init, tgt = synth.workload("small_32x32", seed=25, n_models=24, steps=3000,
+                                              W=40, H=36, min_conc_change=1e-2, fitness=0,
+                                              n_exp=2)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=8)
+        _, _, base_st = ev.evaluate_batch(batch)
+        ev.set_schedule(grn.SCHEDULE_STREAM)
+        raw, states = ev.evaluate_states(batch, max_planes=8)
+        _, _, st = ev.evaluate_batch(batch)
+    assert st["schedule"] == grn.SCHEDULE_STREAM
+    assert st["total_steps"] == base_st["total_steps"] < 24 * 2 * 3000
+    assert np.array_equal(states, base_states)
+    assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream early exit")
+
+
 def test_stream_copy_wait_times_out_cleanly():
     """A bulk copy that never arrives (test hook): the kernel's bounded wait
     runs out after about a second, the call reports it, and the context
