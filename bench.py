@@ -268,6 +268,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--euler-steps", type=int, default=None,
+                    help="override the workload's Euler step count (small profiling cases)")
     ap.add_argument("--schedule", default="auto",
                     choices=["auto", "fixed_items", "walk_items", "global", "cluster", "stream"],
                     help="force a kernel schedule instead of the autotuner's choice")
@@ -311,8 +313,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return t.item()
 
+    over = {"steps": args.euler_steps} if args.euler_steps else {}
     params, batch, init, tgt = synth.workload(args.workload, seed=args.seed + rank,
-                                              n_models=args.models)
+                                              n_models=args.models, **over)
     n = batch.n_models
     ev = grn.Evaluator(params, device=local)
     ev.set_experiments(init, tgt)
