@@ -80,11 +80,25 @@ struct LaunchPlan {
   int band_rows;         // streaming schedule: rows per staged band (else 0)
 };
 
-// Floats of one state plane of a W x H grid: rows padded to float4 groups,
-// plus a zero row above and below (see the kernel's Geom).  With a cluster
-// of C CTAs per model a CTA's plane holds a band of ceil(H / C) rows.
+#ifdef __CUDACC__
+#define GRN_HOST_DEVICE __host__ __device__
+#else
+#define GRN_HOST_DEVICE
+#endif
+
+// Floats of one padded state row: W rounded up to float4 groups, plus one
+// zero group when W is a multiple of 4, so that every row ends in at least
+// one zero cell (the right border of its last cell and the left border of
+// the next row's first cell).
+GRN_HOST_DEVICE inline int row_floats(int W) {
+  return 4 * ((W + 3) / 4) + (W % 4 == 0 ? 4 : 0);
+}
+
+// Floats of one state plane of a W x H grid: padded rows plus a zero row
+// above and below (see the kernel's Geom).  With a cluster of C CTAs per
+// model a CTA's plane holds a band of ceil(H / C) rows.
 inline int64_t plane_floats(int W, int H, int cluster = 1) {
-  return (int64_t)((H + cluster - 1) / cluster + 2) * 4 * ((W + 3) / 4);
+  return (int64_t)((H + cluster - 1) / cluster + 2) * row_floats(W);
 }
 
 // Bytes of shared memory a block needs besides the state planes.

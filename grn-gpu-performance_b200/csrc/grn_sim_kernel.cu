@@ -13,9 +13,10 @@
 //     buffered (one barrier per step) or single buffered with the new values
 //     held in registers (two barriers per step); grids too large for shared
 //     memory use the same code on double-buffered global-memory slots;
-//   - each thread owns float4 groups of 4 cells along x; left/right
-//     neighbours come from warp shuffles (lanes hold consecutive groups),
-//     up/down neighbours from 128-bit loads;
+//   - each thread owns float4 groups of 4 cells along x; up/down
+//     neighbours come from 128-bit loads, left/right ones from 32-bit loads
+//     next to the group (every padded row ends in zero cells, so a row's
+//     borders read 0 without tests);
 //   - regulation is evaluated in exponent form (grn_packed.h): lg2 once per
 //     regulator gene and cell, one FMA + compare/select per link, and
 //     ex2 + rcp once per regulated gene, on the MUFU pipe;
@@ -401,13 +402,15 @@ __device__ __forceinline__ void build_dense(const ModelSmem &M, DenseSmem &D, in
 
 // ---- geometry ----------------------------------------------------------
 //
-// A state plane holds the W x H grid as rows of RS = 4 * Wg floats (rows
-// padded to whole float4 groups) plus one zero row above and one below:
+// A state plane holds the W x H grid as rows of RS = row_floats(W) floats
+// (whole float4 groups, ending in at least one zero cell) plus one zero row
+// above and one below:
 // PS = (H + 2) * RS floats, row y at (y + 1) * RS.  The zero rows make the
 // up/down neighbours of the first and last rows read +0.0, which leaves the
 // reference's neighbour sum unchanged.  Steps write data groups only; when W
 // is not a multiple of 4 the cells past W of a row's last group are written
-// as 0 and serve as that row's right border.
+// as 0, otherwise a zero group ends the row: either way the cell after a
+// row's last cell, and the cell before the next row's first, read 0.
 //
 // A cluster-split launch gives each CTA of a cluster a band of rows
 // [y0, y0 + H) of the Hg-row grid, held the same way: one halo row above and
@@ -424,9 +427,7 @@ struct Item {
   int base;           // float offset of the group in a plane
   float4 tot;         // existing neighbours of each cell (reference `total`)
   bool valid;         // the group exists (an index past the end is clamped
-                      // onto the last group so the lane still shuffles)
-  bool lfix, rfix;    // the neighbour group lives in another warp: read it
-  bool lzero, rzero;  // no neighbour group (grid border)
+                      // onto the last group, computed and not stored)
   bool v1, v2, v3;    // cells 1..3 of the group exist (cell 0 always does)
 };
 
@@ -442,10 +443,7 @@ __device__ __forceinline__ Item make_item(int y, int gx, bool valid, int lane,
   it.tot.y = tv + 1.0f + (x0 + 2 < g.W ? 1.0f : 0.0f);
   it.tot.z = tv + 1.0f + (x0 + 3 < g.W ? 1.0f : 0.0f);
   it.tot.w = tv + 1.0f + (x0 + 4 < g.W ? 1.0f : 0.0f);
-  it.lzero = gx == 0;
-  it.rzero = gx == g.Wg - 1;
-  it.lfix = lane == 0 && !it.lzero;
-  it.rfix = lane == 31 && !it.rzero;
+  (void)lane;
   it.v1 = x0 + 1 < g.W;
   it.v2 = x0 + 2 < g.W;
   it.v3 = x0 + 3 < g.W;
@@ -493,8 +491,8 @@ __device__ __forceinline__ float update_cell(float c, float h, float lim, float 
 }
 
 // New values of one gene for NI groups; `cur` points at the gene's current
-// plane (shared or global memory).  All lanes of a warp call this together
-// (it shuffles).  `mx` takes the max |rate| of the valid groups' real cells.
+// plane (shared or global memory).  `mx` takes the max |rate| of the valid
+// groups' real cells.
 template <int NI, int GMAX, bool EXACT, bool RAGGED>
 __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem &D, int p,
                                             const PackedGene &gn,
@@ -518,12 +516,9 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
       if (diffuses) {
         const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
         const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
-        float lft = __shfl_up_sync(kFull, c.w, 1);
-        float rgt = __shfl_down_sync(kFull, c.x, 1);
-        if (it[i].lfix) lft = cur[it[i].base - 1];
-        if (it[i].rfix) rgt = cur[it[i].base + 4];
-        if (it[i].lzero) lft = 0.0f;
-        if (it[i].rzero) rgt = 0.0f;
+        // Row borders read the zero cells that end every padded row.
+        const float lft = cur[it[i].base - 1];
+        const float rgt = cur[it[i].base + 4];
         // Reference order: x-1, x+1, y-1, y+1.
         const float2 s01 = add2(add2(add2(make_float2(lft, c.x), make_float2(c.y, c.z)),
                                      lo2(up)), lo2(dn));
@@ -556,12 +551,8 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
     if (diffuses) {
       const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
       const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
-      float lft = __shfl_up_sync(kFull, c.w, 1);
-      float rgt = __shfl_down_sync(kFull, c.x, 1);
-      if (it[i].lfix) lft = cur[it[i].base - 1];
-      if (it[i].rfix) rgt = cur[it[i].base + 4];
-      if (it[i].lzero) lft = 0.0f;
-      if (it[i].rzero) rgt = 0.0f;
+      const float lft = cur[it[i].base - 1];  // zero cells at the row borders
+      const float rgt = cur[it[i].base + 4];
       // Reference order: x-1, x+1, y-1, y+1.
       s.x = ((lft + c.y) + up.x) + dn.x;
       s.y = ((c.x + c.z) + up.y) + dn.y;
@@ -942,7 +933,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   g.y0 = rank * Hb;
   g.H = min(A.H - g.y0, Hb);
   g.Wg = A.Wg;
-  g.RS = 4 * A.Wg;
+  g.RS = row_floats(A.W);
   g.PS = (Hb + 2) * g.RS;
   g.Q = g.H * A.Wg;
   const float dt = A.dt, min_conc = A.min_conc;

@@ -68,6 +68,7 @@ struct grn_ctx {
   int smem_optin = 0;
   int n_exp = 0;
   DevBuf d_initial, d_target, d_counter, d_gstate;
+  DevBuf d_sample;  // autotuning: offsets of the sampled records
   Job sync_job;
   std::deque<Job *> pending;
   std::vector<Job *> free_jobs;
@@ -212,7 +213,7 @@ int host_threads() {
 // a multiple of NT / Wg rows keeps every thread busy when Wg divides NT.
 int stream_rows(int W, int H, int gmax, size_t room, int threads) {
   const int Wg = (W + 3) / 4;
-  const size_t row_bytes = (size_t)4 * Wg * sizeof(float);
+  const size_t row_bytes = (size_t)grn::row_floats(W) * sizeof(float);
   long r = (long)(room / (2 * gmax * row_bytes)) - 2;
   r = std::min<long>(r, H);
   while (r > 1 && (size_t)gmax * (r + 2) * row_bytes >= (size_t)1 << 20) --r;
@@ -245,7 +246,8 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace
       if (sched == GRN_SCHEDULE_AUTO && fit / 2 >= max_genes) continue;
       const int R = stream_rows(W, H, v.gmax, optin > fixed ? optin - fixed : 0, v.threads);
       if (R < 1) continue;
-      const size_t smem = fixed + (size_t)2 * v.gmax * (R + 2) * 4 * Wg * sizeof(float);
+      const size_t smem =
+          fixed + (size_t)2 * v.gmax * (R + 2) * grn::row_floats(W) * sizeof(float);
       int per_sm = 0;
       GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &per_sm));
       const int ctas = per_sm * ctx->n_sm;
@@ -400,11 +402,33 @@ grn_status launch_plan(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs a, cud
 // sampled models that the real launch then overwrites.  Synchronises
 // `stream` once per new batch shape.
 grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, LaunchPlan>> &plans,
-                         const grn::SimArgs &a, int n_models, cudaStream_t stream,
-                         LaunchPlan *out) {
+                         const grn::SimArgs &a, int n_models, const int32_t *h_offsets,
+                         cudaStream_t stream, LaunchPlan *out) {
   grn::SimArgs t = a;
-  t.n_models = std::min(n_models, 2 * ctx->n_sm);
-  t.n_steps = std::min(a.n_steps, 64);
+  // About 2^29 cell-updates per sample launch: up to 8 models per SM (so
+  // that, as in the full batch, the slowest block's last model is a small
+  // part of the launch), at least 2 per SM, at least 128 steps (past the
+  // first steps' atypical speed while states are still mostly zero).
+  const double budget = (double)(1u << 29);
+  const double model_cells = (double)a.W * a.H * std::max(1, a.n_exp);
+  const int by_budget = (int)std::min(1e9, budget / (128.0 * model_cells));
+  t.n_models = std::min(n_models, std::max(2 * ctx->n_sm, std::min(8 * ctx->n_sm, by_budget)));
+  t.n_steps = std::min(a.n_steps,
+                       std::max(128, (int)std::min(1e6, budget / (t.n_models * model_cells))));
+  if (h_offsets && n_models > t.n_models) {
+    // Records are in decreasing cost: sample across the whole batch, not
+    // just its most expensive head, so the sample's mix of model sizes is
+    // the batch's.
+    std::vector<int32_t> pick(t.n_models);
+    for (int i = 0; i < t.n_models; ++i)
+      pick[i] = h_offsets[(int64_t)i * n_models / t.n_models];
+    grn_status ss = ensure_dev(ctx, &ctx->d_sample, pick.size() * sizeof(int32_t));
+    if (ss != GRN_OK) return ss;
+    GRN_CUDA(ctx, cudaMemcpyAsync(ctx->d_sample.p, pick.data(), pick.size() * sizeof(int32_t),
+                                  cudaMemcpyHostToDevice, stream));
+    GRN_CUDA(ctx, cudaStreamSynchronize(stream));  // `pick` is pageable and local
+    t.offsets = static_cast<const int32_t *>(ctx->d_sample.p);
+  }
   t.state_out = nullptr;
   t.state_planes = 0;
   const int n_try = std::min<int>((int)plans.size(), 8);
@@ -469,6 +493,8 @@ struct LaunchExtras {
   float *trace = nullptr;   // [model][n_exp][trace_frames][state_planes][H][W]
   int trace_every = 0, trace_frames = 0;
   int experiment = -1;      // >= 0: simulate only this experiment
+  const int32_t *host_offsets = nullptr;  // host copy of the record offsets
+                                          // (autotuning samples across the batch)
 };
 
 // Chooses the plan of a launch of `n_models` packed records already on the
@@ -539,7 +565,7 @@ grn_status prepare_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_o
         }
     }
     if (!found) {
-      s = autotune_plan(ctx, plans, a, n_models, stream, &plan);
+      s = autotune_plan(ctx, plans, a, n_models, ex.host_offsets, stream, &plan);
       if (s != GRN_OK) return s;
       ctx->tuned[key] = grn_ctx::Tuned{plan.v, plan.cluster, plan.planes, 0.0};
     }
@@ -705,11 +731,13 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   GRN_CUDA(ctx, cudaMemsetAsync(j->d_flag.p, 0, 4, st));
   GRN_CUDA(ctx, cudaEventRecord(j->ev_start, st));
   LaunchPlan plan{};
+  LaunchExtras ex;
+  ex.host_offsets = ph.offsets.data();
   s = launch_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
                     static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes, ph.max_links,
                     static_cast<const double *>(j->d_maxerr.p),
                     static_cast<double *>(j->d_raw.p), static_cast<int32_t *>(j->d_steps.p),
-                    static_cast<int32_t *>(j->d_flag.p), st, &plan);
+                    static_cast<int32_t *>(j->d_flag.p), st, &plan, ex);
   if (s != GRN_OK) return s;
   GRN_CUDA(ctx, cudaEventRecord(j->ev_kernel, st));
   GRN_CUDA(ctx, cudaMemcpyAsync(j->h_raw.p, j->d_raw.p, eb, cudaMemcpyDeviceToHost, st));
@@ -824,7 +852,8 @@ grn_status grn_destroy(grn_ctx *ctx) {
     delete j;
   }
   free_job(&ctx->sync_job);
-  for (DevBuf *b : {&ctx->d_initial, &ctx->d_target, &ctx->d_counter, &ctx->d_gstate})
+  for (DevBuf *b : {&ctx->d_initial, &ctx->d_target, &ctx->d_counter, &ctx->d_gstate,
+                    &ctx->d_sample})
     if (b->p) cudaFree(b->p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -996,6 +1025,7 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
                         LaunchExtras x;
                         x.states = static_cast<float *>(d_states.p);
                         x.state_planes = max_planes;
+                        x.host_offsets = ph.offsets.data();
                         return x;
                       }());
     int32_t flag = 0;
@@ -1229,10 +1259,12 @@ grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_ma
   grn_status s = ensure_dev(ctx, &ctx->sync_job.d_flag, 4);
   if (s != GRN_OK) return s;
   GRN_CUDA(ctx, cudaMemsetAsync(ctx->sync_job.d_flag.p, 0, 4, st));
+  LaunchExtras ex;
+  ex.host_offsets = pk->host.offsets.data();
   return launch_packed(ctx, static_cast<const uint4 *>(pk->d_words.p),
                        static_cast<const int32_t *>(pk->d_offsets.p), pk->host.n_models,
                        pk->host.max_genes, pk->host.max_links, d_max_error, d_raw_error, d_steps,
-                       static_cast<int32_t *>(ctx->sync_job.d_flag.p), st, nullptr);
+                       static_cast<int32_t *>(ctx->sync_job.d_flag.p), st, nullptr, ex);
 }
 
 }  // extern "C"

@@ -206,11 +206,13 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size);
 /* GRN_SCHEDULE_AUTO's plan choice.  enable = 1 (default): measured -- on the
  * first batch of each shape (W, H, most genes, most links, experiments,
  * fast path, batch size below 2 x SMs) up to 8 feasible plans are timed on
- * the batch's most expensive models with at most 64 steps (three
- * interleaved rounds after an untimed launch of each; the heuristic's first
- * choice stays unless another plan is 3% faster), and the winner is kept for
- * later batches of that shape (that first call synchronises its stream).  enable = 0: an occupancy/spill heuristic, no timing.  Either
- * call clears the cache. */
+ * a sample of the batch (2 to 8 models per SM, spread evenly over its cost
+ * order; about 2^29 cell-updates per sample launch, at least 128 steps),
+ * in three interleaved rounds after an untimed launch of each; the
+ * heuristic's first choice stays unless another plan is 3% faster.  The winner is kept for later
+ * batches of that shape (that first call synchronises its stream).
+ * enable = 0: an occupancy/spill heuristic, no timing.  Either call clears
+ * the cache. */
 grn_status grn_set_autotune(grn_ctx *ctx, int enable);
 
 /* The last measured autotuning on this context, one line per timed plan
