@@ -20,6 +20,12 @@ cudaError_t mlp_gemm(int M, int N, int K, const __nv_bfloat16 *A, int64_t a_rs, 
                      const __nv_bfloat16 *B, int64_t b_rs, int64_t b_cs, int epi, float *Cf,
                      __nv_bfloat16 *Cb, int64_t ldc, const float *bias,
                      const __nv_bfloat16 *mask, cudaStream_t st);
+// The same GEMM on the tcgen05 tensor cores (grn_umma.cu); sets
+// *error_flag (device) to 1 if a wait for the tensor core timed out.
+cudaError_t mlp_gemm_tc(int M, int N, int K, const __nv_bfloat16 *A, int64_t a_rs, int64_t a_cs,
+                        const __nv_bfloat16 *B, int64_t b_rs, int64_t b_cs, int epi, float *Cf,
+                        __nv_bfloat16 *Cb, int64_t ldc, const float *bias,
+                        const __nv_bfloat16 *mask, int *error_flag, cudaStream_t st);
 cudaError_t mlp_output_forward(int B, int K, const __nv_bfloat16 *h, const float *w,
                                const float *b0, float *y, cudaStream_t st);
 cudaError_t mlp_loss(int B, const float *y, const float *t, float *dy, double *loss,

@@ -161,6 +161,7 @@ _SIGNATURES = {
     "grn_surrogate_train": ([_P, _I, _I, ctypes.c_float, ctypes.POINTER(_D)], _I),
     "grn_surrogate_train_batches": ([_P, _I, _I, ctypes.c_float, ctypes.POINTER(_D)], _I),
     "grn_surrogate_predict": ([_P, _P, _I, _P], _I),
+    "grn_surrogate_use_tcgen05": ([_P, _I], _I),
     "grn_surrogate_params": ([_P, _P, _I], _I),
     "grn_surrogate_set_params": ([_P, _P, _I], _I),
     "grn_surrogate_gradients": ([_P, _P, _P, _I, _P, ctypes.POINTER(_D)], _I),
@@ -663,6 +664,9 @@ class Surrogate:
         _check(self.lib.grn_surrogate_train(self.handle, epochs, batch_size, lr,
                                             ctypes.byref(loss)))
         return loss.value
+
+    def use_tcgen05(self, enable=True):
+        _check(self.lib.grn_surrogate_use_tcgen05(self.handle, int(bool(enable))))
 
     def train_batches(self, n_batches, batch_size=512, lr=1e-3):
         loss = ctypes.c_double()

@@ -55,19 +55,42 @@ struct grn_surrogate {
   float *dt = nullptr;
   int step = 0;
   std::mt19937_64 rng;
+  bool tcgen05 = true;     // GEMMs on tcgen05 (else mma.sync)
+  int *d_err = nullptr;    // set by a tcgen05 GEMM whose wait timed out
 };
 
 namespace {
 
+// One GEMM of the MLP on the selected tensor-core path.
+cudaError_t gemm(grn_surrogate *s, int M, int N, int K, const __nv_bfloat16 *A, int64_t a_rs,
+                 int64_t a_cs, const __nv_bfloat16 *B, int64_t b_rs, int64_t b_cs, int epi,
+                 float *Cf, __nv_bfloat16 *Cb, int64_t ldc, const float *bias,
+                 const __nv_bfloat16 *mask) {
+  if (s->tcgen05)
+    return grn::mlp_gemm_tc(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, epi, Cf, Cb, ldc, bias, mask,
+                            s->d_err, s->st);
+  return grn::mlp_gemm(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, epi, Cf, Cb, ldc, bias, mask,
+                       s->st);
+}
+
+// Reads and clears the tcgen05 time-out flag (after the stream is synced).
+grn_status check_err(grn_surrogate *s) {
+  int e = 0;
+  GRN_CK(cudaMemcpy(&e, s->d_err, sizeof e, cudaMemcpyDeviceToHost));
+  if (!e) return GRN_OK;
+  GRN_CK(cudaMemset(s->d_err, 0, sizeof e));
+  return GRN_ERR_KERNEL;
+}
+
 grn_status forward(grn_surrogate *s, int B) {
   using namespace grn;
   cudaStream_t st = s->st;
-  GRN_CK(mlp_gemm(B, kH, kF, s->x, kF, 1, s->wb + kW1, kF, 1, kEpiBiasRelu, nullptr, s->h1, kH,
-                  s->w + kB1, nullptr, st));
-  GRN_CK(mlp_gemm(B, kH, kH, s->h1, kH, 1, s->wb + kW2, kH, 1, kEpiBiasRelu, nullptr, s->h2, kH,
-                  s->w + kB2, nullptr, st));
-  GRN_CK(mlp_gemm(B, kH, kH, s->h2, kH, 1, s->wb + kW3, kH, 1, kEpiBiasRelu, nullptr, s->h3, kH,
-                  s->w + kB3, nullptr, st));
+  GRN_CK(gemm(s, B, kH, kF, s->x, kF, 1, s->wb + kW1, kF, 1, kEpiBiasRelu, nullptr, s->h1, kH,
+                  s->w + kB1, nullptr));
+  GRN_CK(gemm(s, B, kH, kH, s->h1, kH, 1, s->wb + kW2, kH, 1, kEpiBiasRelu, nullptr, s->h2, kH,
+                  s->w + kB2, nullptr));
+  GRN_CK(gemm(s, B, kH, kH, s->h2, kH, 1, s->wb + kW3, kH, 1, kEpiBiasRelu, nullptr, s->h3, kH,
+                  s->w + kB3, nullptr));
   GRN_CK(mlp_output_forward(B, kH, s->h3, s->w + kW4, s->w + kB4, s->y, st));
   return GRN_OK;
 }
@@ -80,20 +103,20 @@ grn_status backward(grn_surrogate *s, int B) {
   GRN_CK(mlp_output_backward(B, kH, s->h3, s->w + kW4, s->dy, s->g + kW4, s->g + kB4, s->dz3,
                              st));
   // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * [H2 > 0]
-  GRN_CK(mlp_gemm(kH, kH, B, s->dz3, 1, kH, s->h2, 1, kH, kEpiF32, s->g + kW3, nullptr, kH,
-                  nullptr, nullptr, st));
+  GRN_CK(gemm(s, kH, kH, B, s->dz3, 1, kH, s->h2, 1, kH, kEpiF32, s->g + kW3, nullptr, kH,
+                  nullptr, nullptr));
   GRN_CK(mlp_column_sum(B, kH, s->dz3, s->g + kB3, st));
-  GRN_CK(mlp_gemm(B, kH, kH, s->dz3, kH, 1, s->wb + kW3, 1, kH, kEpiMask, nullptr, s->dz2, kH,
-                  nullptr, s->h2, st));
+  GRN_CK(gemm(s, B, kH, kH, s->dz3, kH, 1, s->wb + kW3, 1, kH, kEpiMask, nullptr, s->dz2, kH,
+                  nullptr, s->h2));
   // layer 2
-  GRN_CK(mlp_gemm(kH, kH, B, s->dz2, 1, kH, s->h1, 1, kH, kEpiF32, s->g + kW2, nullptr, kH,
-                  nullptr, nullptr, st));
+  GRN_CK(gemm(s, kH, kH, B, s->dz2, 1, kH, s->h1, 1, kH, kEpiF32, s->g + kW2, nullptr, kH,
+                  nullptr, nullptr));
   GRN_CK(mlp_column_sum(B, kH, s->dz2, s->g + kB2, st));
-  GRN_CK(mlp_gemm(B, kH, kH, s->dz2, kH, 1, s->wb + kW2, 1, kH, kEpiMask, nullptr, s->dz1, kH,
-                  nullptr, s->h1, st));
+  GRN_CK(gemm(s, B, kH, kH, s->dz2, kH, 1, s->wb + kW2, 1, kH, kEpiMask, nullptr, s->dz1, kH,
+                  nullptr, s->h1));
   // layer 1: dW1 = dZ1^T X (no input gradient needed)
-  GRN_CK(mlp_gemm(kH, kF, B, s->dz1, 1, kH, s->x, 1, kF, kEpiF32, s->g + kW1, nullptr, kF,
-                  nullptr, nullptr, st));
+  GRN_CK(gemm(s, kH, kF, B, s->dz1, 1, kH, s->x, 1, kF, kEpiF32, s->g + kW1, nullptr, kF,
+                  nullptr, nullptr));
   GRN_CK(mlp_column_sum(B, kH, s->dz1, s->g + kB1, st));
   return GRN_OK;
 }
@@ -211,6 +234,8 @@ grn_status grn_surrogate_create(int device, uint64_t seed, int capacity, grn_sur
   alloc((void **)&s->idx, B * 4);
   alloc((void **)&s->dx, (size_t)capacity * kF * 2);
   alloc((void **)&s->dt, (size_t)capacity * 4);
+  alloc((void **)&s->d_err, sizeof(int));
+  if (ok && cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess) ok = false;
   if (!ok) {
     grn_surrogate_destroy(s);
     return GRN_ERR_OUT_OF_MEMORY;
@@ -241,7 +266,8 @@ grn_status grn_surrogate_destroy(grn_surrogate *s) {
   for (void *p : {(void *)s->w, (void *)s->g, (void *)s->m, (void *)s->v, (void *)s->wb,
                   (void *)s->x, (void *)s->h1, (void *)s->h2, (void *)s->h3, (void *)s->dz1,
                   (void *)s->dz2, (void *)s->dz3, (void *)s->y, (void *)s->t, (void *)s->dy,
-                  (void *)s->loss, (void *)s->idx, (void *)s->dx, (void *)s->dt})
+                  (void *)s->loss, (void *)s->idx, (void *)s->dx, (void *)s->dt,
+                  (void *)s->d_err})
     if (p) cudaFree(p);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
@@ -309,7 +335,7 @@ grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, flo
     }
   }
   if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
-  return GRN_OK;
+  return check_err(s);
 }
 
 grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batch_size, float lr,
@@ -328,7 +354,7 @@ grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batc
     if (st != GRN_OK) return st;
   }
   if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
-  return GRN_OK;
+  return check_err(s);
 }
 
 grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n, float *out) {
@@ -342,6 +368,12 @@ grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n,
     GRN_CK(cudaMemcpyAsync(out + i, s->y, B * 4, cudaMemcpyDeviceToHost, s->st));
     GRN_CK(cudaStreamSynchronize(s->st));
   }
+  return check_err(s);
+}
+
+grn_status grn_surrogate_use_tcgen05(grn_surrogate *s, int enable) {
+  if (!s) return GRN_ERR_INVALID_ARGUMENT;
+  s->tcgen05 = enable != 0;
   return GRN_OK;
 }
 
@@ -361,7 +393,7 @@ grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
   GRN_CK(cudaMemcpyAsync(&l, s->loss, 8, cudaMemcpyDeviceToHost, s->st));
   GRN_CK(cudaStreamSynchronize(s->st));
   if (loss) *loss = l;
-  return GRN_OK;
+  return check_err(s);
 }
 
 }  // extern "C"

@@ -545,6 +545,11 @@ grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n,
 /* FP32 parameters (GRN_SURROGATE_PARAMS values) out / in (in resets Adam). */
 grn_status grn_surrogate_params(grn_surrogate *s, float *params, int n);
 grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n);
+/* The GEMMs' tensor-core path: 1 (default) tcgen05.mma with the accumulator
+ * in tensor memory; 0 warp-level mma.sync (both BF16 x BF16 -> FP32).
+ * GRN_ERR_KERNEL from a surrogate call means a tcgen05 GEMM's bounded wait
+ * for the tensor core ran out. */
+grn_status grn_surrogate_use_tcgen05(grn_surrogate *s, int enable);
 /* Mean squared loss and its parameter gradients on n pairs, no update. */
 grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
                                    const float *log_error, int n, float *grads, double *loss);

@@ -126,6 +126,27 @@ def test_surrogate_gradients_match_fp64(built_libs):
 
 
 @pytest.mark.gpu
+def test_tcgen05_and_mma_sync_paths_agree(built_libs):
+    """The GEMMs on tcgen05 (accumulator in tensor memory) and on warp-level
+    mma.sync give the same predictions and gradients up to FP32 summation
+    order (and the BF16 roundings it can flip)."""
+    rng = np.random.default_rng(5)
+    s = grn.Surrogate(seed=15)
+    x = rng.normal(size=(333, 128)).astype(np.float32)  # ragged 128-row tiles
+    t = rng.normal(size=333).astype(np.float32)
+    out = {}
+    for tc in (True, False):
+        s.use_tcgen05(tc)
+        out[tc] = (s.predict(x), s.gradients(x, t))
+    (y1, (l1, g1)), (y0, (l0, g0)) = out[True], out[False]
+    assert np.linalg.norm(y1 - y0) <= 2e-3 * np.linalg.norm(y0)
+    assert abs(l1 - l0) <= 1e-3 * abs(l0)
+    b1, b0 = _blocks(g1), _blocks(g0)
+    for name, _ in mlp_ref.SHAPES:
+        assert np.linalg.norm(b1[name] - b0[name]) <= 5e-3 * np.linalg.norm(b0[name]), name
+
+
+@pytest.mark.gpu
 def test_surrogate_adam_step(built_libs):
     rng = np.random.default_rng(2)
     s = grn.Surrogate(seed=12, capacity=256)
