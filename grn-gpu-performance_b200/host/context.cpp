@@ -729,15 +729,20 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   GRN_CUDA(ctx, cudaMemcpyAsync(j->d_offsets.p, j->h_offsets.p, ob, cudaMemcpyHostToDevice, st));
   GRN_CUDA(ctx, cudaMemcpyAsync(j->d_maxerr.p, j->h_maxerr.p, eb, cudaMemcpyHostToDevice, st));
   GRN_CUDA(ctx, cudaMemsetAsync(j->d_flag.p, 0, 4, st));
-  GRN_CUDA(ctx, cudaEventRecord(j->ev_start, st));
+  // Plan first (a new batch shape is autotuned here, on the copied
+  // records), so that the kernel events time the real launch only.
   LaunchPlan plan{};
+  grn::SimArgs a{};
   LaunchExtras ex;
   ex.host_offsets = ph.offsets.data();
-  s = launch_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
-                    static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes, ph.max_links,
-                    static_cast<const double *>(j->d_maxerr.p),
-                    static_cast<double *>(j->d_raw.p), static_cast<int32_t *>(j->d_steps.p),
-                    static_cast<int32_t *>(j->d_flag.p), st, &plan, ex);
+  s = prepare_packed(ctx, static_cast<const uint4 *>(j->d_words.p),
+                     static_cast<const int32_t *>(j->d_offsets.p), n, ph.max_genes,
+                     ph.max_links, static_cast<const double *>(j->d_maxerr.p),
+                     static_cast<double *>(j->d_raw.p), static_cast<int32_t *>(j->d_steps.p),
+                     static_cast<int32_t *>(j->d_flag.p), st, &plan, &a, ex);
+  if (s != GRN_OK) return s;
+  GRN_CUDA(ctx, cudaEventRecord(j->ev_start, st));
+  s = enqueue_plan(ctx, plan, a, st);
   if (s != GRN_OK) return s;
   GRN_CUDA(ctx, cudaEventRecord(j->ev_kernel, st));
   GRN_CUDA(ctx, cudaMemcpyAsync(j->h_raw.p, j->d_raw.p, eb, cudaMemcpyDeviceToHost, st));
