@@ -9,10 +9,10 @@
 //     model from an atomic work counter (the host orders models by cost,
 //     longest first);
 //   - a model's state lives in shared memory for all Euler steps (planar
-//     [gene][y][x] FP32, rows padded to float4 groups), either double
-//     buffered (one barrier per step) or single buffered with the new values
-//     held in registers (two barriers per step); grids too large for shared
-//     memory use the same code on double-buffered global-memory slots;
+//     [gene][y][x] FP32, rows padded to float4 groups), double buffered
+//     (one barrier per step); genes that do not fit use the same code on
+//     double-buffered global-memory slots, and grids too large for shared
+//     memory stream bands of rows through it (or split across a cluster);
 //   - each thread owns float4 groups of 4 cells along x; up/down
 //     neighbours come from 128-bit loads, left/right ones from 32-bit loads
 //     next to the group (every padded row ends in zero cells, so a row's

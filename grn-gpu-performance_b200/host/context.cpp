@@ -475,9 +475,9 @@ grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, Launc
     char line[200];
     std::snprintf(line, sizeof line,
                   "%s schedule %d threads %d gmax %d items %d cluster %d planes %d band %d "
-                  "ms %.4f\n",
+                  "blocks %d ms %.4f\n",
                   i == best ? "*" : " ", p.schedule, p.v.threads, p.v.gmax, p.v.items,
-                  std::max(1, p.cluster), p.planes, p.band_rows, best_ms[i]);
+                  std::max(1, p.cluster), p.planes, p.band_rows, p.blocks, best_ms[i]);
     rep += line;
   }
   ctx->last_tuning = rep;
