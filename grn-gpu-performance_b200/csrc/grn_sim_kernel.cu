@@ -431,8 +431,7 @@ struct Item {
   bool v1, v2, v3;    // cells 1..3 of the group exist (cell 0 always does)
 };
 
-__device__ __forceinline__ Item make_item(int y, int gx, bool valid, int lane,
-                                          const Geom &g) {
+__device__ __forceinline__ Item make_item(int y, int gx, bool valid, const Geom &g) {
   Item it;
   it.valid = valid;
   it.base = (y + 1) * g.RS + 4 * gx;
@@ -443,18 +442,17 @@ __device__ __forceinline__ Item make_item(int y, int gx, bool valid, int lane,
   it.tot.y = tv + 1.0f + (x0 + 2 < g.W ? 1.0f : 0.0f);
   it.tot.z = tv + 1.0f + (x0 + 3 < g.W ? 1.0f : 0.0f);
   it.tot.w = tv + 1.0f + (x0 + 4 < g.W ? 1.0f : 0.0f);
-  (void)lane;
   it.v1 = x0 + 1 < g.W;
   it.v2 = x0 + 2 < g.W;
   it.v3 = x0 + 3 < g.W;
   return it;
 }
 
-__device__ __forceinline__ Item item_at(int q, int lane, const Geom &g) {
+__device__ __forceinline__ Item item_at(int q, const Geom &g) {
   const bool valid = q < g.Q;
   const int qc = valid ? q : g.Q - 1;
   const int y = qc / g.Wg;
-  return make_item(y, qc - y * g.Wg, valid, lane, g);
+  return make_item(y, qc - y * g.Wg, valid, g);
 }
 
 __device__ __forceinline__ int cell_offset(const Geom &g, int y, int x) {
@@ -788,7 +786,7 @@ template <int NT, int GMAX, bool RAGGED>
 __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSmem &D,
                             const StatePtrs &sp, const Geom &g, int G, int par, bool exact,
                             float dt, float min_conc, float &mx, uint64_t *bars,
-                            uint32_t &mphase, int lane) {
+                            uint32_t &mphase) {
   const int R = A.band_rows;
   const int nb = (g.H + R - 1) / R;
   const int SPS = (R + 2) * g.RS;
@@ -830,8 +828,8 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     gb.Q = gb.H * g.Wg;
     const float *st = stage0 + s * GMAX * SPS;
     const int n_it = (gb.Q + NT - 1) / NT;
-    for (int i = 0; i < n_it; ++i) {  // every lane of a warp iterates together (shuffles)
-      const Item it[1] = {item_at(threadIdx.x + i * NT, lane, gb)};
+    for (int i = 0; i < n_it; ++i) {  // the same count in every thread (barriers follow)
+      const Item it[1] = {item_at(threadIdx.x + i * NT, gb)};
       band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st, G, gb, it, gl_nxt, gps, dt,
                                             min_conc, mx);
     }
@@ -958,7 +956,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   Item items[LOOP ? 1 : ITEMS];
   if constexpr (!LOOP) {
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) items[i] = item_at(tid + i * NT, lane, g);
+    for (int i = 0; i < ITEMS; ++i) items[i] = item_at(tid + i * NT, g);
   }
   // Walking items: per-iteration stride (ITEMS * NT groups) in (row, group
   // column).
@@ -1066,7 +1064,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         float mx = 0.0f;
         if constexpr (ST) {
           if (!stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
-                                              bars, mphase, lane)) {
+                                              bars, mphase)) {
             if (tid == 0) {
               atomicExch(A.error_flag, 2);
               A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
@@ -1095,7 +1093,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
               const int q = tid + (i * ITEMS + j) * NT;
-              it[j] = q < g.Q ? make_item(y[j], gx[j], true, lane, g) : item_at(q, lane, g);
+              it[j] = q < g.Q ? make_item(y[j], gx[j], true, g) : item_at(q, g);
             }
             if (exact)
               group_step<ITEMS, GMAX, GMAX, true, RAGGED>(M, D, sp, g, it, par, dt, min_conc,
