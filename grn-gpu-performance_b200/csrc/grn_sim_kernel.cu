@@ -193,9 +193,11 @@ constexpr size_t kWorkOffset = kDredOffset + 32 * 8;     // int [2]
 // step parity) and per-CTA fitness sums double [kMaxCluster].
 constexpr size_t kCmaxOffset = kWorkOffset + 16;
 constexpr size_t kCsumOffset = kCmaxOffset + 2 * kMaxCluster * 4;
-// Two mbarriers of the streaming schedule's copy stages.
+// Two mbarriers of the streaming schedule's copy stages, then its copy
+// time-out flag (int).
 constexpr size_t kMbarOffset = (kCsumOffset + kMaxCluster * 8 + 15) & ~size_t(15);
-constexpr size_t kStateOffset = (kMbarOffset + 16 + 127) & ~size_t(127);
+constexpr size_t kStreamFailOffset = kMbarOffset + 16;
+constexpr size_t kStateOffset = (kStreamFailOffset + 16 + 127) & ~size_t(127);
 
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
 
@@ -782,11 +784,15 @@ __device__ __forceinline__ void band_group_step_any(bool exact, const ModelSmem 
 // band b.  mphase holds each stage's next wait parity across steps.
 // Returns false (the same in every thread) if a copy did not complete in
 // time; the copies still in flight have then been waited for (bounded).
+// A thread whose wait runs out raises *fail and computes its band from
+// whatever the stage holds; the band's one barrier then makes the decision
+// block-wide (the model's results are discarded on that path).  *fail is 0
+// on entry and is never cleared: the kernel returns after a failure.
 template <int NT, int GMAX, bool RAGGED>
 __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSmem &D,
                             const StatePtrs &sp, const Geom &g, int G, int par, bool exact,
                             float dt, float min_conc, float &mx, uint64_t *bars,
-                            uint32_t &mphase) {
+                            uint32_t &mphase, volatile int *fail) {
   const int R = A.band_rows;
   const int nb = (g.H + R - 1) / R;
   const int SPS = (R + 2) * g.RS;
@@ -812,15 +818,8 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
   for (int b = 0; b < nb; ++b) {
     const int s = b & 1;
     const uint32_t parity = (mphase >> s) & 1u;
-    const bool ok = mbar_wait(bars + s, parity);
+    if (!mbar_wait(bars + s, parity)) *fail = 1;
     mphase ^= 1u << s;
-    if (!__syncthreads_and(ok)) {
-      // Bounded second waits for copies that may still be in flight: the
-      // timed-out one (unless withheld) and the one issued ahead.
-      if (!withhold) mbar_wait(bars + s, parity);
-      if (b + 1 < nb) mbar_wait(bars + (s ^ 1), (mphase >> (s ^ 1)) & 1u);
-      return false;
-    }
     Geom gb = g;
     gb.y0 = b * R;
     gb.H = min(R, g.H - b * R);
@@ -833,7 +832,14 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
       band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st, G, gb, it, gl_nxt, gps, dt,
                                             min_conc, mx);
     }
-    __syncthreads();  // stage s is free again
+    __syncthreads();  // stage s is free again; *fail is the same for every thread
+    if (*fail) {
+      // Bounded second waits for copies that may still be in flight: the
+      // timed-out one (unless withheld) and the one issued ahead.
+      if (!withhold) mbar_wait(bars + s, parity);
+      if (b + 1 < nb) mbar_wait(bars + (s ^ 1), (mphase >> (s ^ 1)) & 1u);
+      return false;
+    }
     if (threadIdx.x == 0 && b + 2 < nb) issue(b + 2);
   }
   fence_proxy_async_global();  // this step's writes before the next step's copies
@@ -942,12 +948,14 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   sp.gl = A.gstate ? A.gstate + (size_t)blockIdx.x * (size_t)A.slot_floats : nullptr;
 
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kMbarOffset);
+  volatile int *s_stream_fail = reinterpret_cast<volatile int *>(smem + kStreamFailOffset);
   uint32_t mphase = 0;  // streaming: next wait parity of each stage
   if constexpr (ST) {
     if (tid == 0) {
       mbar_init(bars, 1);
       mbar_init(bars + 1, 1);
       mbar_init_fence();
+      *s_stream_fail = 0;
     }
     __syncthreads();
   }
@@ -1064,7 +1072,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         float mx = 0.0f;
         if constexpr (ST) {
           if (!stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
-                                              bars, mphase)) {
+                                              bars, mphase, s_stream_fail)) {
             if (tid == 0) {
               atomicExch(A.error_flag, 2);
               A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
