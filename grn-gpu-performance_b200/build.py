@@ -7,7 +7,9 @@ CUDA sources are compiled for sm_100a only
 g++; everything links into lib/libgrn_b200.so with the CUDA runtime linked
 statically, so the library loads without a CUDA toolkit on the library path.
 The ptxas resource report (registers, spills, shared memory per kernel) is
-written to _build/ptxas.log.
+written to _build/ptxas.log.  lib/libgrn_b200_checked.so is the same library
+with the simulation kernel built with GRN_BOUNDS_CHECK=1 (every state access
+checked; for the tests).
 """
 import glob
 import os
@@ -20,6 +22,10 @@ ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libgrn_b200.so")
+# The same library with every state access of the simulation kernel
+# bounds-checked (GRN_BOUNDS_CHECK, tests only).
+CHECKED_LIB = os.path.join(LIB_DIR, "libgrn_b200_checked.so")
+KERNEL_SRC = os.path.join(HERE, "csrc", "grn_sim_kernel.cu")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -76,6 +82,15 @@ def build(force=False, verbose=False):
             f.write("\n".join(ptxas_log))
     if force or _newer(LIB, objs):
         _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs
+             + ["-cudart", "static", "-Xcompiler", "-pthread", "-lrt", "-ldl"], verbose)
+    checked_obj = os.path.join(BUILD, "grn_sim_kernel_checked.cu.o")
+    if force or _newer(checked_obj, [KERNEL_SRC] + HEADERS):
+        _run([nvcc] + ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                              "--expt-relaxed-constexpr", "-DGRN_BOUNDS_CHECK=1",
+                              "-c", KERNEL_SRC, "-o", checked_obj], verbose)
+    checked_objs = [checked_obj if o.endswith("grn_sim_kernel.cu.o") else o for o in objs]
+    if force or _newer(CHECKED_LIB, checked_objs):
+        _run([nvcc] + ARCH + ["-shared", "-o", CHECKED_LIB] + checked_objs
              + ["-cudart", "static", "-Xcompiler", "-pthread", "-lrt", "-ldl"], verbose)
     return LIB
 

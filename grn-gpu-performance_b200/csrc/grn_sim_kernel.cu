@@ -37,6 +37,12 @@
 #include "grn_packed.h"
 #include "grn_sim.h"
 
+// GRN_BOUNDS_CHECK=1 builds the bounds-checked library
+// (lib/libgrn_b200_checked.so): every state access is checked (see chk).
+#ifndef GRN_BOUNDS_CHECK
+#define GRN_BOUNDS_CHECK 0
+#endif
+
 namespace grn {
 namespace {
 
@@ -197,9 +203,72 @@ constexpr size_t kCsumOffset = kCmaxOffset + 2 * kMaxCluster * 4;
 // time-out flag (int).
 constexpr size_t kMbarOffset = (kCsumOffset + kMaxCluster * 8 + 15) & ~size_t(15);
 constexpr size_t kStreamFailOffset = kMbarOffset + 16;
-constexpr size_t kStateOffset = (kStreamFailOffset + 16 + 127) & ~size_t(127);
+// Bounds-checked build only: the regions that state accesses are checked
+// against (CheckRegions).
+constexpr size_t kCheckOffset = (kStreamFailOffset + 16 + 15) & ~size_t(15);
+constexpr size_t kCheckBytes = GRN_BOUNDS_CHECK ? 64 : 0;
+constexpr size_t kStateOffset = (kCheckOffset + kCheckBytes + 127) & ~size_t(127);
 
 __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
+
+// ---- bounds-checked build ----------------------------------------------
+//
+// With GRN_BOUNDS_CHECK every state access goes through chk: the N floats
+// at p must lie inside the block's shared-memory state area (from the state
+// offset to the end of the dynamic shared memory) or the launch's global
+// state slots, and a float4 access must be 16-byte aligned.  An access that
+// is not is redirected to a scratch float4 (nothing outside the buffers is
+// touched) and sets the error flag to 3, which the host reports as
+// GRN_ERR_KERNEL.  Without it chk is the identity.  This stands in for a
+// memory checker: the GPU tests run every schedule through the checked
+// library on small grids.
+struct CheckRegions {
+  const float *sm_lo, *sm_hi;  // shared-memory state area
+  const float *gl_lo, *gl_hi;  // global state slots of the whole launch
+  int32_t *flag;
+  float4 scratch;              // target of redirected accesses
+};
+static_assert(sizeof(CheckRegions) <= 64, "check regions fit their slot");
+
+extern __shared__ __align__(128) unsigned char grn_dyn_smem[];
+
+__device__ __forceinline__ bool check_span(const float *p, long n) {
+  const CheckRegions &c = *reinterpret_cast<const CheckRegions *>(grn_dyn_smem + kCheckOffset);
+  return (p >= c.sm_lo && p + n <= c.sm_hi) || (c.gl_lo && p >= c.gl_lo && p + n <= c.gl_hi);
+}
+
+__device__ __forceinline__ void check_failed() {
+  CheckRegions &c = *reinterpret_cast<CheckRegions *>(grn_dyn_smem + kCheckOffset);
+  atomicCAS(c.flag, 0, 3);
+}
+
+template <int N>
+__device__ __forceinline__ float *chk(const float *p) {
+#if GRN_BOUNDS_CHECK
+  const bool aligned = N < 4 || (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+  if (!aligned || !check_span(p, N)) {
+    check_failed();
+    CheckRegions &c = *reinterpret_cast<CheckRegions *>(grn_dyn_smem + kCheckOffset);
+    return reinterpret_cast<float *>(&c.scratch);
+  }
+#endif
+  return const_cast<float *>(p);
+}
+
+// A bulk copy's source and destination spans (floats); false (and the flag)
+// if either leaves its buffer, in which case the copy is not issued.
+__device__ __forceinline__ bool chk_copy(const float *dst, const float *src, long n) {
+#if GRN_BOUNDS_CHECK
+  if (!check_span(dst, n) || !check_span(src, n)) {
+    check_failed();
+    return false;
+  }
+#endif
+  (void)dst;
+  (void)src;
+  (void)n;
+  return true;
+}
 
 // ---- regulation ------------------------------------------------------
 //
@@ -510,15 +579,15 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
     // two cells per FP32 instruction.
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      const float4 c = *reinterpret_cast<const float4 *>(cur + it[i].base);
+      const float4 c = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base));
       float2 r01 = fma2(f2(-gn.deg), lo2(c), mul2(f2(gn.lim), lo2(h[i])));
       float2 r23 = fma2(f2(-gn.deg), hi2(c), mul2(f2(gn.lim), hi2(h[i])));
       if (diffuses) {
-        const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
-        const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
+        const float4 up = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base - g.RS));
+        const float4 dn = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base + g.RS));
         // Row borders read the zero cells that end every padded row.
-        const float lft = cur[it[i].base - 1];
-        const float rgt = cur[it[i].base + 4];
+        const float lft = *chk<1>(cur + it[i].base - 1);
+        const float rgt = *chk<1>(cur + it[i].base + 4);
         // Reference order: x-1, x+1, y-1, y+1.
         const float2 s01 = add2(add2(add2(make_float2(lft, c.x), make_float2(c.y, c.z)),
                                      lo2(up)), lo2(dn));
@@ -546,13 +615,13 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
   }
 #pragma unroll
   for (int i = 0; i < NI; ++i) {
-    const float4 c = *reinterpret_cast<const float4 *>(cur + it[i].base);
+    const float4 c = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base));
     float4 s = f4(0.0f);
     if (diffuses) {
-      const float4 up = *reinterpret_cast<const float4 *>(cur + it[i].base - g.RS);
-      const float4 dn = *reinterpret_cast<const float4 *>(cur + it[i].base + g.RS);
-      const float lft = cur[it[i].base - 1];  // zero cells at the row borders
-      const float rgt = cur[it[i].base + 4];
+      const float4 up = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base - g.RS));
+      const float4 dn = *reinterpret_cast<const float4 *>(chk<4>(cur + it[i].base + g.RS));
+      const float lft = *chk<1>(cur + it[i].base - 1);  // zero cells at the row borders
+      const float rgt = *chk<1>(cur + it[i].base + 4);
       // Reference order: x-1, x+1, y-1, y+1.
       s.x = ((lft + c.y) + up.x) + dn.x;
       s.y = ((c.x + c.z) + up.y) + dn.y;
@@ -657,7 +726,7 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
       const float *pl = (k < sp.n_sm ? sm_cur : gl_cur) + k * g.PS;
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
-        const float4 c = *reinterpret_cast<const float4 *>(pl + it[i].base);
+        const float4 c = *reinterpret_cast<const float4 *>(chk<4>(pl + it[i].base));
         lg[i][k].x = lg2_approx(c.x);
         lg[i][k].y = lg2_approx(c.y);
         lg[i][k].z = lg2_approx(c.z);
@@ -672,7 +741,7 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
                                        mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
-      if (it[i].valid) *reinterpret_cast<float4 *>(sm_nxt + p * g.PS + it[i].base) = nv[i];
+      if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(sm_nxt + p * g.PS + it[i].base)) = nv[i];
   }
   for (int p = sp.n_sm; p < G; ++p) {
     const PackedGene gn = M.genes[p];
@@ -681,7 +750,7 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
                                        mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
-      if (it[i].valid) *reinterpret_cast<float4 *>(gl_nxt + p * g.PS + it[i].base) = nv[i];
+      if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(gl_nxt + p * g.PS + it[i].base)) = nv[i];
   }
 }
 
@@ -736,7 +805,7 @@ __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseS
       const float *pl = stage + k * gb.PS;
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
-        const float4 c = *reinterpret_cast<const float4 *>(pl + it[i].base);
+        const float4 c = *reinterpret_cast<const float4 *>(chk<4>(pl + it[i].base));
         lg[i][k].x = lg2_approx(c.x);
         lg[i][k].y = lg2_approx(c.y);
         lg[i][k].z = lg2_approx(c.z);
@@ -752,7 +821,7 @@ __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseS
                                        min_conc, mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
-      if (it[i].valid) *reinterpret_cast<float4 *>(out + p * gps + it[i].base) = nv[i];
+      if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(out + p * gps + it[i].base)) = nv[i];
   }
 }
 
@@ -806,8 +875,11 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     const uint32_t bytes = (uint32_t)rows * g.RS * 4u;
     fence_proxy_async_shared();
     mbar_expect_tx(bars + (b & 1), bytes * (uint32_t)G);
-    for (int p = 0; p < G; ++p)
-      bulk_g2s(st + p * SPS, gl_cur + p * gps + (size_t)b * R * g.RS, bytes, bars + (b & 1));
+    for (int p = 0; p < G; ++p) {
+      float *dst = st + p * SPS;
+      const float *src = gl_cur + p * gps + (size_t)b * R * g.RS;
+      if (chk_copy(dst, src, (long)rows * g.RS)) bulk_g2s(dst, src, bytes, bars + (b & 1));
+    }
   };
   // Test hook: withhold band 1's copy, so that its wait runs out.
   const bool withhold = A.test_hooks & kHookWithholdBandCopy;
@@ -862,12 +934,14 @@ __device__ __forceinline__ void push_halos(const SimArgs &A, const StatePtrs &sp
     const int dst = dir == 0 ? rank - 1 : rank + 1;
     if (dst < 0 || dst >= C) continue;
     float *pl = plane_of<GMAX>(sp, g, p, nxt);
-    const float4 v = *reinterpret_cast<const float4 *>(pl + (dir == 0 ? 1 : g.H) * g.RS + 4 * c);
+    const float4 v =
+        *reinterpret_cast<const float4 *>(chk<4>(pl + (dir == 0 ? 1 : g.H) * g.RS + 4 * c));
+    const int off = (dir == 0 ? Hb + 1 : 0) * g.RS + 4 * c;
     float *dpl = p < sp.n_sm
-                     ? cl.map_shared_rank(pl, (unsigned)dst)
-                     : A.gstate + (size_t)(blockIdx.x - rank + dst) * (size_t)A.slot_floats +
-                           (pl - sp.gl);
-    *reinterpret_cast<float4 *>(dpl + (dir == 0 ? Hb + 1 : 0) * g.RS + 4 * c) = v;
+                     ? cl.map_shared_rank(chk<4>(pl + off), (unsigned)dst)  // checked locally
+                     : chk<4>(A.gstate + (size_t)(blockIdx.x - rank + dst) * (size_t)A.slot_floats +
+                              (pl - sp.gl) + off);
+    *reinterpret_cast<float4 *>(dpl) = v;
   }
 }
 
@@ -881,7 +955,7 @@ __device__ __forceinline__ void write_planes(const SimArgs &A, const StatePtrs &
     const int kk = i / (g.W * g.H), r = i - kk * g.W * g.H;
     const int y = r / g.W, x = r - y * g.W;
     dst[((size_t)kk * g.Hg + g.y0 + y) * g.W + x] =
-        plane_of<GMAX>(sp, g, kk, par)[cell_offset(g, y, x)];
+        *chk<1>(plane_of<GMAX>(sp, g, kk, par) + cell_offset(g, y, x));
   }
 }
 
@@ -946,6 +1020,20 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
   StatePtrs sp;
   sp.sm = reinterpret_cast<float *>(smem + kStateOffset);
   sp.gl = A.gstate ? A.gstate + (size_t)blockIdx.x * (size_t)A.slot_floats : nullptr;
+
+#if GRN_BOUNDS_CHECK
+  if (tid == 0) {
+    CheckRegions &cr = *reinterpret_cast<CheckRegions *>(smem + kCheckOffset);
+    uint32_t dyn = 0;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    cr.sm_lo = sp.sm;
+    cr.sm_hi = reinterpret_cast<const float *>(smem + dyn);
+    cr.gl_lo = A.gstate;
+    cr.gl_hi = A.gstate ? A.gstate + (size_t)gridDim.x * (size_t)A.slot_floats : nullptr;
+    cr.flag = A.error_flag;
+  }
+  __syncthreads();
+#endif
 
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kMbarOffset);
   volatile int *s_stream_fail = reinterpret_cast<volatile int *>(smem + kStreamFailOffset);
@@ -1049,7 +1137,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         if (kk < A.n_in && y >= 0 && y < g.Hg && x < g.W)
           v = init[((size_t)kk * g.Hg + y) * g.W + x];
         float *pl = plane_of<GMAX>(sp, g, kk, kb < G ? 0 : 1);
-        pl[r] = v;
+        *chk<1>(pl + r) = v;
       }
       if constexpr (ST) fence_proxy_async_global();  // before the first bulk copies
       if constexpr (CL) cg::this_cluster().sync();
@@ -1149,7 +1237,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       for (int i = tid; i < g.W * g.H; i += NT) {
         const int y = i / g.W, x = i - y * g.W;
         for (int kk = 0; kk < A.n_target; ++kk) {
-          const double a = plane_of<GMAX>(sp, g, A.n_in + kk, par)[cell_offset(g, y, x)];
+          const double a = *chk<1>(plane_of<GMAX>(sp, g, A.n_in + kk, par) + cell_offset(g, y, x));
           const double b = tgt[((size_t)kk * g.Hg + g.y0 + y) * g.W + x];
           if (A.fitness_kind == GRN_FITNESS_MSE) {
             acc += (a - b) * (a - b);

@@ -109,11 +109,13 @@ grn_status fail(grn_ctx *ctx, grn_status s, const std::string &msg) {
 }
 
 // The kernel's error flag: 1 a model record it cannot run, 2 a bounded
-// wait for a bulk copy that ran out (streaming schedule).
+// wait for a bulk copy that ran out (streaming schedule), 3 a state access
+// outside its buffer (bounds-checked build only).
 grn_status kernel_flag_error(grn_ctx *ctx, int32_t flag) {
   return fail(ctx, GRN_ERR_KERNEL,
-              flag == 2 ? "the simulation kernel's wait for a bulk copy timed out"
-                        : "the simulation kernel rejected a model record");
+              flag == 3   ? "bounds check: a simulation kernel state access fell outside its buffer"
+              : flag == 2 ? "the simulation kernel's wait for a bulk copy timed out"
+                          : "the simulation kernel rejected a model record");
 }
 
 grn_status cuda_fail(grn_ctx *ctx, cudaError_t e, const char *what) {
