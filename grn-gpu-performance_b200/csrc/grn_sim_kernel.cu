@@ -1086,7 +1086,10 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       const uint4 w0 = rec[0];
       const int G0 = (int)(short)(w0.y & 0xffff);
       const int L0 = (int)(short)(w0.y >> 16);
-      const int words = 1 + G0 + L0;
+      // Counts outside the format's limits: copy the header alone (the model
+      // is rejected below) rather than read past the record.
+      const bool sane = G0 >= 0 && G0 <= GRN_MAX_GENES && L0 >= 0 && L0 <= GRN_MAX_LINKS;
+      const int words = sane ? 1 + G0 + L0 : 1;
       // Header and genes keep their word; links move to ModelSmem::links.
       for (int w = tid; w < words; w += NT) {
         const int dst = (w <= G0) ? w : w - 1 - G0 + 1 + GRN_MAX_GENES;

@@ -32,6 +32,8 @@ SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1
 SCHEDULE_CLUSTER = 4
 SCHEDULE_STREAM = 5
 TEST_WITHHOLD_BAND_COPY = 1
+TEST_FAIL_DEVICE_ALLOC = 2
+TEST_CORRUPT_RECORD = 4
 SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster",
                   5: "stream"}
 

@@ -131,6 +131,8 @@ grn_status cuda_fail(grn_ctx *ctx, cudaError_t e, const char *what) {
 
 grn_status ensure_dev(grn_ctx *ctx, DevBuf *b, size_t bytes) {
   if (bytes <= b->cap) return GRN_OK;
+  if (ctx->test_hooks & GRN_TEST_FAIL_DEVICE_ALLOC)
+    return fail(ctx, GRN_ERR_OUT_OF_MEMORY, "device allocation refused (test hook)");
   if (b->p) cudaFree(b->p);
   b->p = nullptr;
   b->cap = 0;
@@ -716,6 +718,12 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
     GRN_CUDA(ctx, cudaEventCreate(&j->ev_done));
   }
   std::memcpy(j->h_words.p, ph.words.data(), wb);
+  if (ctx->test_hooks & GRN_TEST_CORRUPT_RECORD) {
+    // Gene count 0 in the first record's header (PackedHeader::n_genes).
+    auto *hdr = reinterpret_cast<grn::PackedHeader *>(static_cast<uint4 *>(j->h_words.p) +
+                                                      ph.offsets[0]);
+    hdr->n_genes = 0;
+  }
   std::memcpy(j->h_offsets.p, ph.offsets.data(), ob);
   std::memcpy(j->h_maxerr.p, max_error, eb);
   cudaStream_t st = ctx->stream;
@@ -876,7 +884,9 @@ grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len) {
 }
 
 grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks) {
-  if (!ctx || (hooks & ~GRN_TEST_WITHHOLD_BAND_COPY)) return GRN_ERR_INVALID_ARGUMENT;
+  if (!ctx || (hooks & ~(GRN_TEST_WITHHOLD_BAND_COPY | GRN_TEST_FAIL_DEVICE_ALLOC |
+                         GRN_TEST_CORRUPT_RECORD)))
+    return GRN_ERR_INVALID_ARGUMENT;
   ctx->test_hooks = hooks;
   return GRN_OK;
 }

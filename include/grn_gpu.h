@@ -236,6 +236,13 @@ grn_status grn_set_graphs(grn_ctx *ctx, int enable);
  * the model's raw error becomes NaN and the call returns GRN_ERR_KERNEL; the
  * context stays usable.  0 restores normal operation. */
 #define GRN_TEST_WITHHOLD_BAND_COPY 1
+/* GRN_TEST_FAIL_DEVICE_ALLOC: every device allocation the context would make
+ * fails, so the call returns GRN_ERR_OUT_OF_MEMORY; buffers it already holds
+ * stay usable.  GRN_TEST_CORRUPT_RECORD: the first compiled model record of
+ * each call reaches the kernel with a gene count of 0, which the kernel's
+ * record check rejects (GRN_ERR_KERNEL, that model's raw error NaN). */
+#define GRN_TEST_FAIL_DEVICE_ALLOC 2
+#define GRN_TEST_CORRUPT_RECORD 4
 grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks);
 
 /* ------------------------------------------------------------ experiments */

@@ -321,6 +321,46 @@ def test_stream_copy_wait_times_out_cleanly():
     np.testing.assert_array_equal(raw, want)
 
 
+def test_device_allocation_failure_is_reported_and_recoverable():
+    """Injected on the host: every device allocation of the context fails
+    (test hook).  The call returns GRN_ERR_OUT_OF_MEMORY instead of
+    aborting, and once allocation works again the same context gives the
+    same results as a fresh one."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=26, n_models=20, steps=30,
+                                              W=40, H=30)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        _, want, _ = ev.evaluate_batch(batch)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_test_hooks(grn.TEST_FAIL_DEVICE_ALLOC)
+        with pytest.raises(grn.GrnError) as e:
+            ev.evaluate_batch(batch)
+        assert e.value.status == 4  # GRN_ERR_OUT_OF_MEMORY
+        ev.set_test_hooks(0)
+        _, raw, _ = ev.evaluate_batch(batch)
+    np.testing.assert_array_equal(raw, want)
+
+
+def test_corrupt_record_is_rejected_by_the_kernel():
+    """Injected on the host: the first compiled record reaches the kernel
+    with a gene count of 0 (test hook).  The kernel's record check rejects
+    it without touching memory past the record, the call returns
+    GRN_ERR_KERNEL, and the context keeps working."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=27, n_models=20, steps=30,
+                                              W=40, H=30)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        _, want, _ = ev.evaluate_batch(batch)
+        ev.set_test_hooks(grn.TEST_CORRUPT_RECORD)
+        with pytest.raises(grn.GrnError) as e:
+            ev.evaluate_batch(batch)
+        assert e.value.status == 10 and "rejected a model record" in str(e.value)
+        ev.set_test_hooks(0)
+        _, raw, _ = ev.evaluate_batch(batch)
+    np.testing.assert_array_equal(raw, want)
+
+
 def test_cluster_schedule_rejects_empty_bands():
     params, batch, init, tgt = synth.workload("small_32x32", seed=17, n_models=4, steps=10,
                                               W=32, H=20)
