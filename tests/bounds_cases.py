@@ -43,6 +43,24 @@ def run_cases():
         for sched in (grn.SCHEDULE_FIXED_ITEMS, grn.SCHEDULE_WALK_ITEMS, grn.SCHEDULE_GLOBAL):
             _states(out, "grid%dx%d_s%d" % (W, H, sched), params, batch, init, tgt, sched,
                     planes=8)
+    # Degenerate grids: one cell, one column, one row, one float4 group per
+    # row (the zero group that ends it), every schedule including streaming.
+    for W, H in ((1, 1), (1, 37), (53, 1), (4, 9)):
+        params, batch, init, tgt = synth.workload("uneven_64x64", seed=9, n_models=6, steps=12,
+                                                  W=W, H=H)
+        for sched in (grn.SCHEDULE_FIXED_ITEMS, grn.SCHEDULE_WALK_ITEMS, grn.SCHEDULE_GLOBAL,
+                      grn.SCHEDULE_STREAM):
+            _states(out, "edge%dx%d_s%d" % (W, H, sched), params, batch, init, tgt, sched,
+                    planes=8)
+    # Clusters whose bands are one row high (halo rows only) and a short last band.
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=10, n_models=4, steps=12,
+                                              W=17, H=2)
+    _states(out, "cluster17x2_c2", params, batch, init, tgt, grn.SCHEDULE_CLUSTER, cluster=2,
+            planes=8)
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=11, n_models=4, steps=12,
+                                              W=9, H=7)
+    _states(out, "cluster9x7_c4", params, batch, init, tgt, grn.SCHEDULE_CLUSTER, cluster=4,
+            planes=8)
     # 100x100 walking: 2 genes on chip, the rest in global slots.
     params, batch, init, tgt = synth.workload("islands_100x100", seed=4, n_models=10, steps=20)
     _states(out, "islands_walk", params, batch, init, tgt, grn.SCHEDULE_WALK_ITEMS, planes=8)
