@@ -9,8 +9,12 @@
 // grn_evaluate_batch, but everything the kernel needs beyond the caller's
 // inputs and outputs -- the work counter, the error flag, the compiled model
 // records and the per-block state slots of genes that do not fit in shared
-// memory -- lives in one file-scope device array of GRN_NOALLOC_SCRATCH_BYTES
-// that the library reserves once per GPU.
+// memory -- lives in one file-scope device array of GRN_NOALLOC_SCRATCH_BYTES.
+// The array is reserved on a GPU when this module is loaded there; with
+// CUDA's lazy module loading (the default) that is the first call on that
+// device, which looks the array's address up.  A caller that divides the
+// device memory itself should make that first call (a call with no models
+// is enough) before it does.
 //
 // The array is shared by every call on a device and keeps the previous
 // call's contents; each call clears the counter and flag it relies on (the
@@ -34,7 +38,8 @@
 namespace grn {
 namespace {
 
-// Reserved once per GPU that loads the library, for the life of the process.
+// Reserved on each GPU when the module loads there, for the life of the
+// process.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[GRN_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
@@ -57,6 +62,13 @@ cudaError_t scratch_address(int device, void **out) {
 }
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// The scratch array starts with the kernel's work counter and error flag.
+constexpr size_t kFlagOffset = sizeof(int32_t);
+
+grn_status cuda_status(cudaError_t e) {
+  return e == cudaErrorMemoryAllocation ? GRN_ERR_OUT_OF_MEMORY : GRN_ERR_CUDA;
+}
 
 grn_status put_error(char *buf, int len, grn_status s, const std::string &msg) {
   if (buf && len > 0) {
@@ -83,19 +95,21 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
       params->n_target_morphogens < 0 || params->n_target_morphogens > 3 ||
       (params->fitness_kind != GRN_FITNESS_REF_LOGTHRESH && params->fitness_kind != GRN_FITNESS_MSE))
     return put_error(err_buf, err_buf_len, GRN_ERR_INVALID_ARGUMENT, "bad simulation parameters");
-  if (batch->n_models == 0) return GRN_OK;
-  if (!batch->product_offsets || !batch->link_offsets || batch->product_offsets[0] != 0 ||
-      batch->link_offsets[0] != 0)
-    return put_error(err_buf, err_buf_len, GRN_ERR_INVALID_ARGUMENT, "bad batch offsets");
 
+  // Set-up first, even for an empty batch: looking the array up loads the
+  // module, which reserves the array on this device.
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
     return put_error(err_buf, err_buf_len, GRN_ERR_NO_DEVICE, "no current CUDA device");
   void *scratch = nullptr;
   cudaError_t e = scratch_address(device, &scratch);
   if (e != cudaSuccess)
-    return put_error(err_buf, err_buf_len, GRN_ERR_CUDA,
+    return put_error(err_buf, err_buf_len, cuda_status(e),
                      std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  if (batch->n_models == 0) return GRN_OK;
+  if (!batch->product_offsets || !batch->link_offsets || batch->product_offsets[0] != 0 ||
+      batch->link_offsets[0] != 0)
+    return put_error(err_buf, err_buf_len, GRN_ERR_INVALID_ARGUMENT, "bad batch offsets");
 
   // Compile the batch on the host (host memory only).
   PackedHost ph;
@@ -177,7 +191,7 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
     e = cudaMemcpyAsync(base + offs_off, ph.offsets.data(), offs_bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(base, 0, 2 * sizeof(int32_t), st);  // counter, flag
   if (e != cudaSuccess)
-    return put_error(err_buf, err_buf_len, GRN_ERR_CUDA,
+    return put_error(err_buf, err_buf_len, cuda_status(e),
                      std::string("copy into scratch: ") + cudaGetErrorString(e));
 
   SimArgs a{};
@@ -206,14 +220,42 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
   a.raw_error = d_raw_error;
   a.steps = d_steps;
   a.work_counter = reinterpret_cast<int32_t *>(base);
-  a.error_flag = reinterpret_cast<int32_t *>(base) + 1;
+  a.error_flag = reinterpret_cast<int32_t *>(base + kFlagOffset);
   if (best.slot_floats > 0) {
     a.gstate = reinterpret_cast<float *>(base + slots_off);
     a.slot_floats = best.slot_floats;
   }
   e = sim_launch(best, a, st);
   if (e != cudaSuccess)
-    return put_error(err_buf, err_buf_len, GRN_ERR_CUDA,
+    return put_error(err_buf, err_buf_len, cuda_status(e),
                      std::string("kernel launch: ") + cudaGetErrorString(e));
   return GRN_OK;
+}
+
+extern "C" grn_status grn_evaluate_batch_noalloc_status(void *cuda_stream, char *err_buf,
+                                                        int err_buf_len) {
+  using namespace grn;
+  if (err_buf && err_buf_len > 0) err_buf[0] = '\0';
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
+    return put_error(err_buf, err_buf_len, GRN_ERR_NO_DEVICE, "no current CUDA device");
+  void *scratch = nullptr;
+  cudaError_t e = scratch_address(device, &scratch);
+  if (e != cudaSuccess)
+    return put_error(err_buf, err_buf_len, cuda_status(e),
+                     std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  int32_t flag = 0;
+  e = cudaMemcpyAsync(&flag, static_cast<unsigned char *>(scratch) + kFlagOffset, sizeof flag,
+                      cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess)
+    return put_error(err_buf, err_buf_len, cuda_status(e),
+                     std::string("reading the error flag: ") + cudaGetErrorString(e));
+  if (flag == 0) return GRN_OK;
+  return put_error(err_buf, err_buf_len, GRN_ERR_KERNEL,
+                   flag == 3   ? "bounds check: a simulation kernel state access fell outside "
+                                 "its buffer"
+                   : flag == 2 ? "the simulation kernel's wait for a bulk copy timed out"
+                               : "the simulation kernel rejected a model record");
 }

@@ -34,11 +34,13 @@ constexpr int kConstSlot = 255;
 
 // Header flags.
 constexpr uint32_t kFlagNone = 0u;
-// Every link has a finite K > 0 and a finite Hill coefficient, every gene
-// finite rates, and no (regulator, regulated) pair repeats: on a
-// non-negative finite state no link term can be NaN, so the kernel may
-// combine terms with min/max over a dense per-gene table of regulator slots
-// (see the kernel's regulation).
+// Every link has a finite K > 0, a finite Hill coefficient n <= 32 and
+// 0 < K^n <= 1e300, every gene finite rates, and no (regulator, regulated)
+// pair repeats: on a bounded non-negative state no link term can be NaN, so
+// the kernel may combine terms with min/max over a dense per-gene table of
+// regulator slots (see the kernel's regulation).  The kernel also requires
+// the step size to keep the state bounded (euler_bounded) before it takes
+// the fast path.
 constexpr uint32_t kFlagFast = 1u;
 
 struct alignas(16) PackedHeader {

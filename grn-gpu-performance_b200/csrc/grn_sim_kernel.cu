@@ -275,9 +275,10 @@ __device__ __forceinline__ bool chk_copy(const float *dst, const float *src, lon
 // A gene's regulation is 1 / (1 + 2^V), V combined in exponent space over
 // its links (grn_packed.h).  Two combine modes:
 //   fast   min / max (fminf / fmaxf).  Identical to the reference whenever
-//          no link term is NaN, which the host guarantees for models with
-//          finite K > 0 and finite Hill coefficients on non-negative finite
-//          states (flag kFlagFast).
+//          no link term is NaN, which holds for models with finite K > 0,
+//          finite Hill coefficients and 0 < K^n <= 1e300 (flag kFlagFast) on
+//          bounded non-negative states (euler_bounded and the host's
+//          fast_ok).
 //   exact  the reference's comparison order (simopor.cpp:20-22,
 //          simopand.cpp:20-22 with MathAlgo::max/min): a NaN term on
 //          either side yields the new term; a NaN start makes the first
@@ -528,6 +529,31 @@ __device__ __forceinline__ Item item_at(int q, const Geom &g) {
 
 __device__ __forceinline__ int cell_offset(const Geom &g, int y, int x) {
   return (y + 1) * g.RS + x;
+}
+
+// Whether a fast-flagged model may run the fast path at this step size.
+// The fast path needs a state that stays finite and non-negative.  With
+// dt >= 0, deg >= 0 and dt*(deg + 4*dif) <= 1 for every gene, the explicit
+// Euler update of a cell is a combination with non-negative weights of its
+// old value, its neighbours and dt*lim*h (h in [0, 1]), so no value goes
+// negative and the largest value grows by at most dt*max(lim, 0) per step.
+// Bounding that growth over the run (kFastMaxGrowth) and the initial state
+// (the host's fast_ok) keeps every x^n and K^n far from overflow.  A model
+// outside the bound -- an unstable step such as dt*dif > 1/4, where a
+// checkerboard mode grows until cells overflow to inf and NaN -- runs the
+// exact path, which keeps the reference's inf / NaN behaviour
+// (modelsimulator.cpp:262-275, simstate.cpp:147-151).
+constexpr float kFastMaxGrowth = 1.0e6f;
+
+__device__ __forceinline__ bool euler_bounded(const ModelSmem &M, int G, float dt,
+                                              int n_steps) {
+  bool ok = dt >= 0.0f;
+  for (int p = 0; p < G; ++p) {
+    const PackedGene &gn = M.genes[p];
+    ok = ok && gn.deg >= 0.0f && dt * (gn.deg + 4.0f * gn.dif) <= 1.0f &&
+         (float)n_steps * dt * fmaxf(gn.lim, 0.0f) <= kFastMaxGrowth;
+  }
+  return ok;
 }
 
 // Euler update of one cell (modelsimulator.cpp:224-275).
@@ -1100,7 +1126,8 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
     const int G = M.hdr.n_genes;
     const int orig = M.hdr.orig_index;
     sp.n_sm = min(G, A.planes / 2);
-    const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast));
+    const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast) &&
+                         G <= GRN_MAX_GENES && euler_bounded(M, G, A.dt, A.n_steps));
     const bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
                      M.hdr.n_links > GRN_MAX_LINKS || (sp.n_sm < G && sp.gl == nullptr) ||
                      (!LOOP && n_iter_band > ITEMS) ||

@@ -135,6 +135,7 @@ _SIGNATURES = {
     "grn_packed_free": ([_P], _I),
     "grn_packed_get_info": ([_P, ctypes.POINTER(PackedInfo)], _I),
     "grn_run_packed": ([_P, _P, _P, _P, _P, _P], _I),
+    "grn_run_packed_status": ([_P, _P], _I),
     "grn_describe_model": ([_P, _I, _P, _I, _I, ctypes.c_char_p, _I], _I),
     "grn_evolution_create": ([ctypes.POINTER(EvolutionParams), _I, _P, ctypes.POINTER(_P)], _I),
     "grn_evolution_create_cb": ([ctypes.POINTER(EvolutionParams), _I, CALCULATOR_FN, _P,
@@ -172,6 +173,7 @@ _SIGNATURES = {
     "grn_evaluate_batch_noalloc": ([ctypes.POINTER(SimParams), _I, _P, _P,
                                     ctypes.POINTER(ModelBatchC), _P, _P, _P, _P,
                                     ctypes.c_char_p, _I], _I),
+    "grn_evaluate_batch_noalloc_status": ([_P, ctypes.c_char_p, _I], _I),
 }
 
 _lib = None
@@ -297,6 +299,18 @@ def evaluate_batch_noalloc(params, n_experiments, d_initial, d_target, batch, d_
                                         ctypes.c_void_p(d_raw_error),
                                         ctypes.c_void_p(d_steps) if d_steps else None,
                                         ctypes.c_void_p(stream) if stream else None, buf, len(buf))
+    if st != GRN_OK:
+        raise GrnError(st, buf.value.decode())
+
+
+def evaluate_batch_noalloc_status(stream=None):
+    """grn_evaluate_batch_noalloc_status: waits for `stream` and raises
+    GrnError (GRN_ERR_KERNEL) if the last no-allocation call's kernel flagged
+    an error."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(512)
+    st = lib.grn_evaluate_batch_noalloc_status(ctypes.c_void_p(stream) if stream else None, buf,
+                                               len(buf))
     if st != GRN_OK:
         raise GrnError(st, buf.value.decode())
 
@@ -453,6 +467,12 @@ class Packed:
                                           ctypes.c_void_p(d_steps) if d_steps else None,
                                           ctypes.c_void_p(stream) if stream is not None else None),
                self.ev.ctx)
+
+    def status(self, stream=None):
+        """grn_run_packed_status: waits for `stream` and raises GrnError
+        (GRN_ERR_KERNEL) if a launch flagged an error since the last call."""
+        _check(self.ev.lib.grn_run_packed_status(
+            self.ev.ctx, ctypes.c_void_p(stream) if stream is not None else None), self.ev.ctx)
 
     def free(self):
         if self.handle:

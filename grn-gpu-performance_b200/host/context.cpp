@@ -69,6 +69,9 @@ struct grn_ctx {
   int n_exp = 0;
   DevBuf d_initial, d_target, d_counter, d_gstate;
   DevBuf d_sample;  // autotuning: offsets of the sampled records
+  // grn_run_packed's error flag: sticky across launches, read and cleared by
+  // grn_run_packed_status.
+  DevBuf d_packed_flag;
   Job sync_job;
   std::deque<Job *> pending;
   std::vector<Job *> free_jobs;
@@ -88,9 +91,10 @@ struct grn_ctx {
   };
   std::map<std::array<int, 7>, Tuned> tuned;
   std::string last_tuning;  // the last autotuning's candidates and times
-  // minConc is 0 and the uploaded initial states are finite and
-  // non-negative: the kernel's fast path then gives the same results as the
-  // exact one (see the kernel's update_cell).
+  // minConc is 0 and the uploaded initial states are finite, non-negative
+  // and at most 1e6: the kernel's fast path then gives the same results as
+  // the exact one for every model whose step size keeps its state bounded
+  // (see the kernel's update_cell and euler_bounded).
   bool fast_ok = false;
 };
 
@@ -868,7 +872,7 @@ grn_status grn_destroy(grn_ctx *ctx) {
   }
   free_job(&ctx->sync_job);
   for (DevBuf *b : {&ctx->d_initial, &ctx->d_target, &ctx->d_counter, &ctx->d_gstate,
-                    &ctx->d_sample})
+                    &ctx->d_sample, &ctx->d_packed_flag})
     if (b->p) cudaFree(b->p);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -944,10 +948,13 @@ grn_status grn_set_experiments(grn_ctx *ctx, int n_experiments, const double *in
                                         cudaMemcpyHostToDevice, ctx->stream));
   GRN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->n_exp = n_experiments;
+  // The fast path's bound on the state (the kernel's euler_bounded) also
+  // needs the initial values below kFastMaxInitial.
+  constexpr double kFastMaxInitial = 1.0e6;
   bool ok = ctx->p.min_conc == 0.0;
   for (size_t i = 0; ok && i < ni; ++i) {
     const double v = fi[i];  // the value the kernel starts from
-    ok = std::isfinite(v) && v >= 0;
+    ok = std::isfinite(v) && v >= 0 && v <= kFastMaxInitial;
   }
   ctx->fast_ok = ok;
   return GRN_OK;
@@ -1273,15 +1280,30 @@ grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_ma
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null device pointer");
   cudaSetDevice(ctx->device);
   cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->stream;
-  grn_status s = ensure_dev(ctx, &ctx->sync_job.d_flag, 4);
-  if (s != GRN_OK) return s;
-  GRN_CUDA(ctx, cudaMemsetAsync(ctx->sync_job.d_flag.p, 0, 4, st));
+  if (!ctx->d_packed_flag.p) {
+    // The flag starts at 0 and stays set until grn_run_packed_status reads it.
+    grn_status s = ensure_dev(ctx, &ctx->d_packed_flag, 4);
+    if (s != GRN_OK) return s;
+    GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_packed_flag.p, 0, 4, st));
+  }
   LaunchExtras ex;
   ex.host_offsets = pk->host.offsets.data();
   return launch_packed(ctx, static_cast<const uint4 *>(pk->d_words.p),
                        static_cast<const int32_t *>(pk->d_offsets.p), pk->host.n_models,
                        pk->host.max_genes, pk->host.max_links, d_max_error, d_raw_error, d_steps,
-                       static_cast<int32_t *>(ctx->sync_job.d_flag.p), st, nullptr, ex);
+                       static_cast<int32_t *>(ctx->d_packed_flag.p), st, nullptr, ex);
+}
+
+grn_status grn_run_packed_status(grn_ctx *ctx, void *cuda_stream) {
+  if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
+  if (!ctx->d_packed_flag.p) return GRN_OK;  // nothing launched yet
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->stream;
+  int32_t flag = 0;
+  GRN_CUDA(ctx, cudaMemcpyAsync(&flag, ctx->d_packed_flag.p, 4, cudaMemcpyDeviceToHost, st));
+  GRN_CUDA(ctx, cudaMemsetAsync(ctx->d_packed_flag.p, 0, 4, st));
+  GRN_CUDA(ctx, cudaStreamSynchronize(st));
+  return flag != 0 ? kernel_flag_error(ctx, flag) : GRN_OK;
 }
 
 }  // extern "C"

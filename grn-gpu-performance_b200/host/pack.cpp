@@ -116,6 +116,15 @@ grn_status pack_model(const grn_product *products, int n_products,
       if (!std::isfinite(n) || !(lk->dis_const > 0) || !std::isfinite(lk->dis_const) ||
           !std::isfinite((float)(n * std::log2(lk->dis_const))))
         hdr.flags &= ~kFlagFast;
+      // The reference computes K^n once in FP64 (simophillact.cpp:9-12) and
+      // then x^n / (x^n + K^n): a K^n that underflows to 0 or overflows makes
+      // 0/0 or inf/inf there, which the exponent form would not reproduce.
+      // With n <= 32 and a bounded state (the kernel's euler_bounded) x^n
+      // stays below 1e202, so x^n + K^n is finite when K^n <= 1e300.
+      if (n > 0) {
+        const double kn = std::pow(lk->dis_const, n);
+        if (!(kn > 0) || !(kn <= 1e300) || n > 32) hdr.flags &= ~kFlagFast;
+      }
       if (n == 0) {
         pl.slot = kConstSlot;  // pow(x, 0) = pow(K, 0) = 1: Hill value 1/2
         pl.a = 0.0f;

@@ -354,6 +354,18 @@ grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *packed,
                           const double *d_max_error, double *d_raw_error,
                           int32_t *d_steps, void *cuda_stream);
 
+/* Waits for the work queued on `cuda_stream` (NULL = the context's stream)
+ * and reports whether a grn_run_packed launch of this context flagged an
+ * internal error since the previous call: GRN_ERR_KERNEL (grn_last_error
+ * says which: a model record the kernel could not run, a bulk-copy wait that
+ * timed out, or a bounds-check failure in the checked library), else GRN_OK.
+ * The flag is one word per context, shared by launches on every stream, and
+ * this call clears it.  A model the kernel rejected also gets a NaN raw
+ * error.  The synchronous entry points (grn_evaluate_batch ...) read their
+ * own flag and need no such call.  No reference counterpart: the reference
+ * aborts the process on any CUDA error (cerrorhandle.h:21). */
+grn_status grn_run_packed_status(grn_ctx *ctx, void *cuda_stream);
+
 /* Compiles one model on the host, as grn_pack does, and writes a text
  * listing of its program (no device work):
  *   "model genes G links L lg_mask M\n"
@@ -573,8 +585,11 @@ grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
 
 /* ------------------------------------------------ no-allocation entry ---
  * Device memory that grn_evaluate_batch_noalloc uses instead of allocating:
- * reserved once on every GPU that loads the library and held until the
- * process exits. */
+ * one array per GPU, reserved when the library's module is loaded on that
+ * GPU and held until the process exits.  Under CUDA's lazy module loading
+ * (the default) the module loads at the first grn_evaluate_batch_noalloc
+ * call on a device; a caller that divides the device memory itself makes
+ * that first call (one with no models is enough) before it does. */
 #define GRN_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* Batch evaluation that allocates no device memory.  No counterpart in the
@@ -607,8 +622,9 @@ grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
  * Every call shares the array and it keeps the previous call's contents;
  * the call clears what must start at zero.  Calls whose GPU work overlaps
  * (other streams, or other threads) race on the array: serialise them.
- * A model record the kernel rejects yields a NaN raw error.  Uses the
- * kernel's exact arithmetic path only.  err_buf (may be NULL) receives a
+ * A model record the kernel rejects yields a NaN raw error, and the
+ * kernel's error flag, which grn_evaluate_batch_noalloc_status reads.  Uses
+ * the kernel's exact arithmetic path only.  err_buf (may be NULL) receives a
  * one-line description of a failure. */
 grn_status grn_evaluate_batch_noalloc(const grn_sim_params *params, int n_experiments,
                                       const float *d_initial, const float *d_target,
@@ -616,6 +632,15 @@ grn_status grn_evaluate_batch_noalloc(const grn_sim_params *params, int n_experi
                                       const double *d_max_error, double *d_raw_error,
                                       int32_t *d_steps, void *cuda_stream,
                                       char *err_buf, int err_buf_len);
+
+/* Waits for `cuda_stream` and reads the error flag that the last
+ * grn_evaluate_batch_noalloc call on the current device left in the scratch
+ * array: GRN_ERR_KERNEL with a description in err_buf if the kernel flagged
+ * an error (a model record it could not run, or a bounds-check failure in
+ * the checked library), else GRN_OK.  The next call clears the flag.  Like
+ * the evaluation it allocates nothing. */
+grn_status grn_evaluate_batch_noalloc_status(void *cuda_stream, char *err_buf,
+                                             int err_buf_len);
 
 /* Rounds a raw error the way the reference's evaluate does:
  * 100 if raw > max_error, else ceilS(raw, precision)

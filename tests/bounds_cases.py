@@ -1,9 +1,9 @@
 """Cases run through both the normal and the bounds-checked library
 (lib/libgrn_b200_checked.so) by tests/test_bounds_checked.py: every kernel
 schedule on small grids -- fixed and walking items, all-global, streaming,
-cluster-split with shared-memory and global-slot genes, trace frames --
-including ragged widths, short last bands, 16-gene models and the exact
-path.
+cluster-split with shared-memory and global-slot genes, trace frames, the
+no-allocation entry's scratch layout -- including ragged widths, short last
+bands, 16-gene models and the exact path.
 
 Run as a script it loads the library named on the command line and writes
 the results to an .npz: python tests/bounds_cases.py LIB OUT.npz
@@ -92,6 +92,23 @@ def run_cases():
         frames, labels = ev.trace(prods, links, every=7, max_frames=8, max_planes=8)
     out["trace/frames"] = frames
     out["trace/labels"] = labels
+    # The no-allocation entry: records, offsets and the state slots of the
+    # genes that spill (7-8 gene models at 64 x 64) in its fixed scratch
+    # array, with its own slot layout and a capped block count.
+    import torch
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=12, n_models=24, steps=15,
+                                              genes=(7, 8))
+    d_init = torch.tensor(init, dtype=torch.float32, device="cuda")
+    d_tgt = torch.tensor(tgt, dtype=torch.float32, device="cuda")
+    d_me = torch.full((batch.n_models,), 1000.0, dtype=torch.float64, device="cuda")
+    d_raw = torch.zeros(batch.n_models, dtype=torch.float64, device="cuda")
+    d_steps = torch.zeros(batch.n_models, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    grn.evaluate_batch_noalloc(params, init.shape[0], d_init.data_ptr(), d_tgt.data_ptr(), batch,
+                               d_me.data_ptr(), d_raw.data_ptr(), d_steps.data_ptr())
+    grn.evaluate_batch_noalloc_status()  # raises on a bounds-check flag
+    out["noalloc/raw"] = d_raw.cpu().numpy()
+    out["noalloc/steps"] = d_steps.cpu().numpy()
     return out
 
 

@@ -1,0 +1,139 @@
+"""GPU parity pinned to the reference itself: the CUDA path, called through
+the C ABI the way a reference caller would use it -- model strings parsed by
+grn_model_parse, experiments uploaded as RGB images by
+grn_set_experiments_rgb -- against the outputs of the reference's own CPU
+fitness path (oracle/_ref, compiled from its unchanged sources):
+
+  - the committed reference-produced fixtures (tests/golden/ref_pinned.json);
+  - the live reference library on the full 64-model 32x32 500-step
+    configuration and on a sample of the 64x64 uneven configuration at its
+    full 2000 steps (skipped where oracle/_ref was not shipped).
+
+Tolerance (the kernels keep FP32 state, the reference FP64): raw errors
+within RTOL = 1e-4 relative (ATOL = 1e-7) of the reference's error, which is
+itself rounded up to error_precision significant digits, so one unit of that
+digit is allowed on top; rounded errors equal to the reference's or within
+that bound; 100 (abandoned) exactly where the reference gives 100; identical
+rankings of ties-free populations; final states within 1e-4 relative +
+1e-6 absolute per cell, with NaN exactly where the reference has NaN.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import grn_b200 as grn
+import ref_binding as ref
+import ref_golden
+import synth
+from grn_b200 import ModelBatch
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+ATOL = 1e-7
+
+
+def _unit(r, precision):
+    return 10.0 ** (math.ceil(math.log10(abs(r))) - precision) if r and np.isfinite(r) else 0.0
+
+
+def assert_errors_match(rounded, raw, want, precision, what):
+    for i, (g, a, r) in enumerate(zip(rounded, raw, want)):
+        if r == 100.0 or g == 100.0:
+            assert g == r, (what, i, g, r)
+            continue
+        if np.isnan(r):
+            assert np.isnan(g), (what, i, g, r)
+            continue
+        tol = ATOL + RTOL * abs(r) + 1.001 * _unit(r, precision)
+        assert abs(a - r) <= tol, (what, i, "raw", a, r)
+        assert abs(g - r) <= tol, (what, i, "rounded", g, r)
+
+
+def assert_same_ranking(got, want):
+    o = np.argsort(want, kind="stable")
+    w, g = want[o], got[o]
+    for i in range(len(w) - 1):
+        for j in range(i + 1, len(w)):
+            if w[j] - w[i] > 2 * RTOL * max(abs(w[i]), abs(w[j])) + ATOL:
+                assert g[i] < g[j], (o[i], o[j], w[i], w[j], g[i], g[j])
+
+
+def assert_states_match(got, want, what):
+    got = got.astype(np.float64)
+    nan_w, nan_g = np.isnan(want), np.isnan(got)
+    assert np.array_equal(nan_w, nan_g), (what, "NaN cells", nan_w.sum(), nan_g.sum())
+    ok = nan_w | (np.abs(got - want) <= 1e-6 + 1e-4 * np.abs(want)) | (got == want)
+    if not ok.all():
+        k, y, x = np.unravel_index(np.argmin(ok), ok.shape)
+        raise AssertionError("%s: gene %d cell (%d,%d): gpu %r reference %r"
+                             % (what, k, x, y, got[k, y, x], want[k, y, x]))
+
+
+def _evaluate(case):
+    p = case["params"]
+    batch = ModelBatch.from_models([grn.parse_model(t) for t in case["models"]])
+    with grn.Evaluator(p) as ev:
+        ev.set_experiments_rgb(case["input_px"], case["target_px"])
+        rounded, raw, _ = ev.evaluate_batch(batch, case["max_error"])
+        runs = [r["model"] for r in case["runs"]]
+        _, states = ev.evaluate_states(batch.subset(runs), case["max_error"][runs],
+                                       max_planes=16)
+    return batch, rounded, raw, states
+
+
+@pytest.mark.parametrize("case", ref_golden.load_cases(), ids=lambda c: c["name"])
+def test_cuda_matches_reference_fixtures(case):
+    p = case["params"]
+    _, rounded, raw, states = _evaluate(case)
+    assert_errors_match(rounded, raw, case["errors"], p["error_precision"], case["name"])
+    finite = np.isfinite(case["errors"]) & (case["errors"] != 100.0)
+    if case["name"] != "unstable_dt":
+        assert_same_ranking(raw[finite], case["errors"][finite])
+    for i, run in enumerate(case["runs"]):
+        n = run["state"].shape[0]
+        assert_states_match(states[i, 0, :n], run["state"], "%s model %d" % (case["name"],
+                                                                              run["model"]))
+
+
+def test_cuda_early_exit_steps_match_reference():
+    case = [c for c in ref_golden.load_cases() if c["name"] == "early_exit"][0]
+    import torch
+    batch = ModelBatch.from_models([grn.parse_model(t) for t in case["models"]])
+    runs = [r["model"] for r in case["runs"]]
+    sub = batch.subset(runs)
+    with grn.Evaluator(case["params"]) as ev:
+        ev.set_experiments_rgb(case["input_px"], case["target_px"])
+        pk = ev.pack(sub)
+        d_me = torch.full((sub.n_models,), 1000.0, dtype=torch.float64, device="cuda")
+        d_raw = torch.zeros(sub.n_models, dtype=torch.float64, device="cuda")
+        d_steps = torch.zeros(sub.n_models, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        pk.run(d_me.data_ptr(), d_raw.data_ptr(), d_steps.data_ptr())
+        pk.status()
+        steps = d_steps.cpu().numpy()
+        pk.free()
+    assert steps.tolist() == [r["steps"] for r in case["runs"]]
+
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref was not shipped")
+
+
+@needs_ref
+@pytest.mark.parametrize("name,n_models,kw", [
+    ("small_32x32", 64, dict(fitness=0)),   # the full configuration, reference fitness
+    ("uneven_64x64", 48, dict()),           # a sample at the full 2000 steps
+])
+def test_cuda_matches_reference_library(name, n_models, kw):
+    params, batch, init, tgt = synth.workload(name, seed=91, n_models=n_models, **kw)
+    ipx = np.stack([ref.encode_rgb(e) for e in init])
+    tpx = np.stack([ref.encode_rgb(e) for e in tgt])
+    want = ref.evaluate_batch(params, ipx, tpx, batch, n_threads=16)
+    texts = ref.batch_texts(batch)
+    parsed = ModelBatch.from_models([grn.parse_model(t) for t in texts])
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments_rgb(ipx, tpx)
+        rounded, raw, _ = ev.evaluate_batch(parsed)
+    assert_errors_match(rounded, raw, want, params["error_precision"], name)
+    assert_same_ranking(raw, want)
