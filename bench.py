@@ -125,28 +125,64 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(workload, seed, budget_s=15.0, threads=None):
-    """Times the FP64 oracle on a bounded sample of the workload: one model
-    per host thread per round, full Euler steps, rounds until ~budget_s."""
+def _ref_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import binding as oracle  # oracle = the CPU baseline only
+    import ref_binding  # the reference's own CPU path (oracle/_ref): baseline only
+    return ref_binding
+
+
+def cpu_baseline(workload, seed, budget_s=15.0, threads=None, euler_steps=None):
+    """Times the reference's CPU fitness path on the host cores, on a bounded
+    sample of the workload: one model per host thread per round, full Euler
+    steps (or `euler_steps`), rounds until ~budget_s.
+
+    It is the reference's own code -- EvaluatorMorphogens on Simulator /
+    ModelSimulator, compiled from its unchanged sources into
+    oracle/_ref/libgrn_ref_o3.so (-O3 -march=x86-64-v3) -- run by a pool of
+    threads with one evaluator each, as its CPU calculator threads run.  It
+    takes the experiments as RGB images (its input format) and has only its
+    thresholded-log fitness.  Where oracle/_ref was not shipped, the FP64
+    restatement (oracle port) stands in for it."""
     threads = threads or os.cpu_count() or 1
-    params, batch, init, tgt = synth.workload(workload, seed=seed + 1000,
-                                              n_models=max(threads, 1))
-    t0 = time.perf_counter()
-    oracle.evaluate_batch(params, init, tgt, batch.subset([0]), n_threads=1)
-    t1 = time.perf_counter() - t0
+    over = {"steps": euler_steps} if euler_steps else {}
+    ref = _ref_module()
+    if ref.available(timed=True) or ref.available():
+        timed = ref.available(timed=True)
+
+        def run(n, n_threads):
+            params, batch, init, tgt = synth.workload(workload, seed=seed + 1000, n_models=n,
+                                                      **over)
+            params = dict(params, fitness_kind=0)
+            ipx = np.stack([ref.encode_rgb(e) for e in init])
+            tpx = np.stack([ref.encode_rgb(e) for e in tgt])
+            texts = ref.batch_texts(batch)
+            t0 = time.perf_counter()
+            ref.evaluate_texts(params, ipx, tpx, texts, n_threads=n_threads, timed=timed)
+            return time.perf_counter() - t0, params
+        kind = "reference"
+        build = ("oracle/_ref/libgrn_ref_o3.so (-O3 -march=x86-64-v3)" if timed else
+                 "oracle/_ref/libgrn_ref.so (-O2)")
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import binding as oracle  # the FP64 port: baseline only
+
+        def run(n, n_threads):
+            params, batch, init, tgt = synth.workload(workload, seed=seed + 1000, n_models=n,
+                                                      **over)
+            t0 = time.perf_counter()
+            oracle.evaluate_batch(params, init, tgt, batch, n_threads=n_threads)
+            return time.perf_counter() - t0, params
+        kind = "port"
+        build = "oracle/_build/libgrn_oracle.so (FP64 restatement, -O2)"
+    t1, _ = run(1, 1)
     rounds = max(1, min(8, int(budget_s / max(t1, 1e-3))))
     n = threads * rounds
-    params, batch, init, tgt = synth.workload(workload, seed=seed + 1000, n_models=n)
-    t0 = time.perf_counter()
-    oracle.evaluate_batch(params, init, tgt, batch, n_threads=threads)
-    dt = time.perf_counter() - t0
+    dt, params = run(n, threads)
     cells = params["dim_x"] * params["dim_y"] * params["num_sim_steps"] * n
-    return {"value": n / dt, "unit": "evals/s", "cores": threads, "kind": "port",
-            "sample": "%d models of %s (full %d steps), %d threads, %.1f s"
-                      % (n, workload, params["num_sim_steps"], threads, dt),
-            "cell_updates_per_s": cells / dt}
+    return {"value": n / dt, "unit": "evals/s", "cores": threads, "kind": kind,
+            "sample": "%d models of %s (%d Euler steps), %d threads, %.1f s; %s"
+                      % (n, workload, params["num_sim_steps"], threads, dt, build),
+            "cell_updates_per_s": cells / dt, "seconds": dt}
 
 
 def run_reference(args, rank, world):
@@ -165,17 +201,123 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": "GRN fitness evals/sec", "value": value,
         "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * statistics.mean(
-            float(v["sample"].split(", ")[-1].split()[0]) for v in vals),
+        "ms_per_step": 1000.0 * statistics.mean(v["seconds"] for v in vals),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": args.workload, "models": wl["n_models"],
                    "grid": "%dx%d" % (wl["W"], wl["H"]), "euler_steps": wl["steps"]},
-        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
-                         "sample": vals[-1]["sample"]},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads,
+                         "kind": vals[-1]["kind"], "sample": vals[-1]["sample"]},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "cell_updates_per_s": statistics.mean(v["cell_updates_per_s"] for v in vals),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _search_arm(grn, ev, evo_p, n_morph, gens, surrogate=None, audit=False, sur_kw=None,
+                score=None):
+    """One seeded island search: per generation (elapsed wall s, best error,
+    stats)."""
+    evo = grn.Evolution(evo_p, n_morph, evaluator=ev)
+    evo.set_skip_clones(True)
+    if surrogate is not None:
+        evo.set_surrogate(surrogate, **(sur_kw or {}))
+        if score is not None:
+            evo.set_surrogate_score(score)
+        if audit:
+            evo.set_surrogate_audit(True)
+    out, t0 = [], time.perf_counter()
+    for _ in range(gens):
+        st = evo.step()
+        out.append((time.perf_counter() - t0, st["best_error"], st))
+    evo.close()
+    return out
+
+
+def run_surrogate_ablation(args, rank, world):
+    """Surrogate-assisted against plain island evolution on the same seed
+    (islands_100x100: 16 demes x 512, 100x100, 1500 Euler steps; both arms
+    skip exact clones).  The surrogate MLP (128 -> 256 x 3 -> 1, BF16
+    tcgen05 GEMMs, FP32 accumulate) trains online on every simulated
+    (model, error) pair of its run (a 200k-pair ring), and from the
+    generation its set holds `min_train` pairs it ranks every generation's
+    children and only the best 25% are simulated.
+    value = wall-clock seconds of the plain run to reach its final best error
+    within 1%, divided by the surrogate run's seconds to reach that same
+    error (null if it never does): > 1 means the surrogate run got there
+    faster.  A second, audited surrogate run (every child simulated, the
+    search unchanged) reports the screen's recall; it is not timed."""
+    if rank != 0:
+        return
+    import torch
+    import grn_b200 as grn
+    torch.cuda.set_device(0)
+    wl = synth.WORKLOADS[args.workload]
+    params = synth.sim_params(wl)
+    init, tgt = synth.experiments(wl, args.seed)
+    n_demes, deme = 16, (args.models or wl["n_models"]) // 16
+    evo_p = dict(n_demes=n_demes, deme_size=deme, migration_period=10, n_max_products=8,
+                 n_max_links=24, n_host_threads=0, seed=args.seed)
+    n_morph = wl["n_in"] + wl["n_target"]
+    gens = args.warmup + args.steps
+    sur_kw = dict(simulate_fraction=0.25, min_train_pairs=args.min_train,
+                  batches_per_generation=32, batch_size=512, lr=1e-3)
+    ev = grn.Evaluator(params)
+    ev.set_experiments(init, tgt)
+    plain = _search_arm(grn, ev, evo_p, n_morph, gens)
+    sur = grn.Surrogate(seed=args.seed, capacity=200000)
+    score = {"paired": grn.SCORE_PAIRED, "parent": grn.SCORE_PARENT_ERROR}[args.score]
+    screened = _search_arm(grn, ev, evo_p, n_morph, gens, sur, sur_kw=sur_kw, score=score)
+    sur.close()
+    audit = None
+    if args.audit:
+        sur2 = grn.Surrogate(seed=args.seed, capacity=200000)
+        audit = _search_arm(grn, ev, evo_p, n_morph, gens, sur2, audit=True, sur_kw=sur_kw,
+                            score=score)
+        sur2.close()
+    ev.close()
+    target = plain[-1][1] * 1.01
+
+    def reach(run):
+        for t, b, _ in run:
+            if b <= target:
+                return t
+        return None
+
+    t_plain, t_sur = reach(plain), reach(screened)
+
+    def summary(run):
+        sims = sum(st["n_evaluated"] for _, _, st in run)
+        rows = [st for _, _, st in run if st["n_screened"] > 0]
+        mean = (lambda k: float(np.nanmean([r[k] for r in rows])) if rows and
+                np.isfinite([r[k] for r in rows]).any() else None)
+        return {"seconds": run[-1][0], "ms_per_generation": 1000 * run[-1][0] / len(run),
+                "final_best_error": run[-1][1], "simulations": sims,
+                "time_to_target_s": reach(run),
+                "best_by_generation": [round(b, 6) for _, b, _ in run],
+                "screened_generations": len(rows),
+                "surrogate_rho_mean": mean("surrogate_rho"),
+                "surrogate_recall_mean": mean("surrogate_recall"),
+                "surrogate_improver_recall_mean": mean("surrogate_improver_recall"),
+                "surrogate_ms_per_generation": float(np.mean([st["surrogate_ms"]
+                                                              for _, _, st in run]))}
+    line = {
+        "metric": "surrogate vs plain evolution: wall-clock to equal best fitness",
+        "value": (t_plain / t_sur) if (t_plain and t_sur) else None, "unit": "x",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32/bf16",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "demes": n_demes, "deme_size": deme,
+                   "grid": "%dx%d" % (wl["W"], wl["H"]), "euler_steps": wl["steps"],
+                   "generations": gens, "skip_clones": True,
+                   "surrogate": "128-256-256-256-1 ReLU MLP, BF16 tcgen05, online, 200k ring, "
+                                "top 25%% simulated from %d pairs" % args.min_train,
+                   "score": args.score,
+                   "target": "plain run's final best error x 1.01"},
+        "target_error": target,
+        "plain": summary(plain), "surrogate": summary(screened),
+        "audit": summary(audit) if audit else None,
     }
     print(json.dumps(line), flush=True)
 
@@ -276,6 +418,23 @@ def main():
     ap.add_argument("--pipeline", action="store_true",
                     help="island workloads: two deme halves alternate on the GPU while the "
                          "host breeds the other (same populations)")
+    ap.add_argument("--shard", action="store_true",
+                    help="split one batch over the ranks through sharded.deal and all-gather "
+                         "the errors (the default when WORLD_SIZE > 1; with one rank it runs "
+                         "the same path on a one-rank process group)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the large_256x256 sub-record of the default workload")
+    ap.add_argument("--large-steps", type=int, default=500,
+                    help="Euler steps of the large_256x256 sub-record (the configuration: 5000)")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="islands_100x100: surrogate-screened against plain evolution, same seed")
+    ap.add_argument("--audit", action="store_true",
+                    help="with --surrogate: a third, audited run that measures the screen's recall")
+    ap.add_argument("--score", default="paired", choices=["paired", "parent"],
+                    help="with --surrogate: rank children by predicted change against the "
+                         "predicted (paired) or the simulated (parent) parent error")
+    ap.add_argument("--min-train", type=int, default=8192,
+                    help="with --surrogate: pairs the surrogate holds before it screens")
     ap.add_argument("--skip-clones", action="store_true",
                     help="island workloads: accept children whose simulated program equals "
                          "their parent's without simulating them")
@@ -288,6 +447,9 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.workload == "islands_100x100" and args.surrogate:
+        run_surrogate_ablation(args, rank, world)
+        return
     if args.workload == "islands_100x100":
         run_evolution(args, rank, world)
         return
@@ -297,9 +459,13 @@ def main():
     import grn_b200 as grn
 
     torch.cuda.set_device(local)
-    if world > 1:
+    sharded_run = world > 1 or args.shard
+    if sharded_run:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        dist.init_process_group("nccl", rank=rank, world_size=world,
+                                timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
     def barrier():
@@ -314,8 +480,24 @@ def main():
         return t.item()
 
     over = {"steps": args.euler_steps} if args.euler_steps else {}
-    params, batch, init, tgt = synth.workload(args.workload, seed=args.seed + rank,
-                                              n_models=args.models, **over)
+    if sharded_run:
+        # One global batch (the same seed on every rank), dealt to the ranks
+        # by compiled cost (sharded.deal); every rank evaluates its shard and
+        # the errors are all-gathered.  Per-GPU work stays at the workload's
+        # model count: weak scaling.
+        import sharded
+        n_per_gpu = args.models or synth.WORKLOADS[args.workload]["n_models"]
+        params, gbatch, init, tgt = synth.workload(args.workload, seed=args.seed,
+                                                   n_models=n_per_gpu * world, **over)
+        n_morph = params["n_input_morphogens"] + params["n_target_morphogens"]
+        ranks = sharded.deal(grn.model_costs(gbatch, n_morph), world)
+        mine = np.nonzero(ranks == rank)[0]
+        batch = gbatch.subset(mine)
+        shard_max = int(np.bincount(ranks, minlength=world).max())
+    else:
+        params, batch, init, tgt = synth.workload(args.workload, seed=args.seed,
+                                                  n_models=args.models, **over)
+        gbatch = batch
     n = batch.n_models
     ev = grn.Evaluator(params, device=local)
     ev.set_experiments(init, tgt)
@@ -332,14 +514,22 @@ def main():
     # "the context's own stream").
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
+    if sharded_run:
+        gather_buf = torch.zeros(shard_max, dtype=torch.float64, device="cuda")
+        gather_parts = [torch.empty_like(gather_buf) for _ in range(world)]
 
     def launch():
         pk.run(me.data_ptr(), raw.data_ptr(), steps_out.data_ptr(), stream.cuda_stream)
+        if sharded_run:
+            # The step's only exchange: every rank's raw errors to every rank.
+            gather_buf[:n].copy_(raw)
+            dist.all_gather(gather_parts, gather_buf)
 
     for _ in range(args.warmup):
         flush.fill_(1)
         launch()
     torch.cuda.synchronize()
+    pk.status(stream.cuda_stream)  # a kernel error flag raises here
 
     # ---- device-resident timing (value) ----
     sampler = ClockSampler(local) if rank == 0 else None
@@ -358,6 +548,7 @@ def main():
         evs.append((e0, e1))
     torch.cuda.synchronize()
     barrier()
+    pk.status(stream.cuda_stream)
     launch_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(sum(launch_ms))
     clocks = sampler.stop() if sampler else None
@@ -367,21 +558,33 @@ def main():
     # ---- end-to-end through the C ABI with host buffers (e2e) ----
     e2e_times = []
     stats = None
+    api = sharded.ShardedEvaluator(ev, n_morph) if sharded_run else ev
     for i in range(max(1, args.warmup // 2) + args.steps):
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        err, rawh, stats = ev.evaluate_batch(batch)
+        err, rawh, stats = api.evaluate_batch(gbatch)
         t1 = time.perf_counter()
         if i >= max(1, args.warmup // 2):
             e2e_times.append(t1 - t0)
     e2e_s = max_over_ranks(sum(e2e_times))
     assert np.isfinite(rawh).all()
-    np.testing.assert_array_equal(rawh, raw.cpu().numpy())
+    if sharded_run:
+        np.testing.assert_array_equal(rawh[mine], raw.cpu().numpy())
+        full = torch.cat(gather_parts).cpu().numpy()
+        order = np.concatenate([np.nonzero(ranks == r)[0] for r in range(world)])
+        starts = np.arange(world) * shard_max
+        counts = np.bincount(ranks, minlength=world)
+        got = np.concatenate([full[starts[r]:starts[r] + counts[r]] for r in range(world)])
+        np.testing.assert_array_equal(got, rawh[order])
+    else:
+        np.testing.assert_array_equal(rawh, raw.cpu().numpy())
+    g_models = gbatch.n_models
 
     if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
+        pk.free()
+        ev.close()
+        dist.destroy_process_group()
         return
 
     peaks, peak_kind = read_peaks()
@@ -399,7 +602,7 @@ def main():
     peak = SFU_PER_CLK_PER_SM * n_sm * sm_max * 1e6 / 1e9
     fp32_peak = FP32_PER_CLK_PER_SM * n_sm * sm_max * 1e6 / 1e9
     prof = read_profile(args.workload)
-    value = n * world * args.steps / (total_ms / 1000.0)
+    value = g_models * args.steps / (total_ms / 1000.0)
     line = {
         "metric": "GRN fitness evals/sec",
         "value": value,
@@ -414,7 +617,7 @@ def main():
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": args.workload, "models_per_gpu": n,
+            "workload": args.workload, "models_per_gpu": n, "models_total": g_models,
             "grid": "%dx%d" % (params["dim_x"], params["dim_y"]),
             "genes": "%d-%d" % synth.WORKLOADS[args.workload]["genes"],
             "links": "%d-%d" % synth.WORKLOADS[args.workload]["links"],
@@ -423,17 +626,20 @@ def main():
             "fitness": ["ref_logthresh", "mse"][params["fitness_kind"]],
             "state": "fp32, fitness sums fp64",
             "l2": "256 MiB buffer written between timed launches (outside the launch events)",
-            "schedule": grn.SCHEDULE_NAMES.get(stats["schedule"], stats["schedule"]),
-            "threads_per_block": stats["threads_per_block"], "blocks": stats["blocks"],
-            "parallelism": "independent batch per GPU" if world > 1 else "1 GPU",
+            "schedule": grn.SCHEDULE_NAMES.get(stats.get("schedule"), stats.get("schedule")),
+            "threads_per_block": stats.get("threads_per_block"), "blocks": stats.get("blocks"),
+            "parallelism": ("one batch dealt over %d GPUs by compiled cost, errors all-gathered "
+                            "(NCCL) every step" % world) if sharded_run else "1 GPU",
         },
         "cell_updates_per_s": steps_run * cells * world * args.steps / (total_ms / 1000.0),
         "e2e": {
-            "value": n * world * args.steps / e2e_s,
+            "value": g_models * args.steps / e2e_s,
             "unit": "evals/s",
-            "h2d_bytes_per_step": int(stats["h2d_bytes"]),
-            "d2h_bytes_per_step": int(stats["d2h_bytes"]),
-            "host_pack_ms": round(stats["pack_ms"], 3),
+            "h2d_bytes_per_step": int(stats.get("h2d_bytes", 0)),
+            "d2h_bytes_per_step": int(stats.get("d2h_bytes", 0)),
+            "host_pack_ms": round(stats.get("pack_ms", 0.0), 3),
+            "api": "sharded.ShardedEvaluator.evaluate_batch" if sharded_run else
+                   "grn_evaluate_batch",
         },
         "roofline": {
             "bound": "sfu",
@@ -457,13 +663,83 @@ def main():
     if clocks and clocks.get("sm_mhz"):
         line["roofline"]["frac_at_sampled_clock"] = achieved / (
             SFU_PER_CLK_PER_SM * n_sm * clocks["sm_mhz"] * 1e6 / 1e9)
-    if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(args.workload, args.seed)
-    print(json.dumps(line), flush=True)
     pk.free()
     ev.close()
-    if world > 1:
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.workload, args.seed)
+    if not args.no_secondary and world == 1 and args.workload == "uneven_64x64":
+        line["secondary"] = [secondary_large(args, grn, torch, local, peaks, peak_kind, n_sm)]
+        line["gpu_launches"] += line["secondary"][0]["gpu_launches"]
+    print(json.dumps(line), flush=True)
+    if sharded_run:
         dist.destroy_process_group()
+
+
+def secondary_large(args, grn, torch, local, peaks, peak_kind, n_sm):
+    """The large-grid stress configuration as a sub-record: large_256x256
+    (1024 models, 8 genes, 24 links, 256x256, dt 0.05) at args.large_steps
+    Euler steps instead of 5000, so that the default run stays short.  Its
+    state (2 x 8 planes of 256 x 256 per model) does not fit on chip; the
+    bound is HBM: algorithmic bytes per cell-update = 2 x 8 genes x 4 B / T,
+    T = Euler steps fused per pass over the state (the plan's temporal
+    blocking depth)."""
+    wl = "large_256x256"
+    params, batch, init, tgt = synth.workload(wl, seed=args.seed, steps=args.large_steps)
+    n = batch.n_models
+    ev = grn.Evaluator(params, device=local)
+    ev.set_experiments(init, tgt)
+    pk = ev.pack(batch)
+    me = torch.full((n,), 1000.0, dtype=torch.float64, device="cuda")
+    raw = torch.zeros(n, dtype=torch.float64, device="cuda")
+    steps_out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(2):  # the first launch autotunes the plan
+        pk.run(me.data_ptr(), raw.data_ptr(), steps_out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    launches = 3
+    evs = []
+    for _ in range(launches):  # 1024 x 2 x 8 x 256 x 256 x 4 B of state > L2
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pk.run(me.data_ptr(), raw.data_ptr(), steps_out.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    pk.status(stream.cuda_stream)
+    ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    _, _, stats = ev.evaluate_batch(batch.subset(range(8)))
+    plan = ev.autotune_report().splitlines()[-1] if ev.autotune_report() else ""
+    pk.free()
+    ev.close()
+    cells = params["dim_x"] * params["dim_y"]
+    cu = int(steps_out.sum().item()) * cells / (ms / 1000.0)
+    genes, t_fused = 8, 1
+    alg_bytes = 2 * genes * 4 / t_fused
+    achieved = cu * alg_bytes / 1e9
+    prof = read_profile(wl)
+    traffic = None
+    if prof and prof.get("dram_bytes_per_cell_update"):
+        traffic = prof["dram_bytes_per_cell_update"] * n * args.large_steps * cells
+    rec = {
+        "config": {"workload": wl, "models": n, "grid": "256x256", "genes": 8, "links": 24,
+                   "euler_steps": args.large_steps, "euler_steps_full": 5000, "dt": 0.05,
+                   "l2": "state of the batch (4.3 GB) exceeds L2"},
+        "metric": "GRN fitness evals/sec", "unit": "evals/s",
+        "value": n / (ms / 1000.0),
+        "value_at_full_steps": cu / (cells * 5000),
+        "cell_updates_per_s": cu, "ms_per_launch": ms, "gpu_launches": launches + 2,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs", 6545.0),
+                     "algorithmic": "%d B per cell-update (2 x %d genes x 4 B, T=%d)" % (
+                         alg_bytes, genes, t_fused),
+                     "traffic": traffic, "peak_source": "%s hbm_gbs" % peak_kind},
+        "plan": plan,
+    }
+    if not args.no_cpu_baseline:
+        rec["cpu_baseline"] = cpu_baseline(wl, args.seed, budget_s=8.0,
+                                           euler_steps=args.large_steps)
+    return rec
 
 
 if __name__ == "__main__":

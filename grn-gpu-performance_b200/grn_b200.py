@@ -34,6 +34,7 @@ SCHEDULE_STREAM = 5
 TEST_WITHHOLD_BAND_COPY = 1
 TEST_FAIL_DEVICE_ALLOC = 2
 TEST_CORRUPT_RECORD = 4
+SCORE_PARENT_ERROR, SCORE_PAIRED = 0, 1
 SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster",
                   5: "stream"}
 
@@ -69,7 +70,9 @@ class GenerationStats(ctypes.Structure):
                 ("host_ms", ctypes.c_double), ("eval_ms", ctypes.c_double),
                 ("migrated", ctypes.c_int32), ("n_screened", ctypes.c_int32),
                 ("surrogate_ms", ctypes.c_double), ("surrogate_loss", ctypes.c_double),
-                ("n_clones", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
+                ("n_clones", ctypes.c_int32), ("n_audited", ctypes.c_int32),
+                ("surrogate_rho", ctypes.c_double), ("surrogate_recall", ctypes.c_double),
+                ("surrogate_improver_recall", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
@@ -170,6 +173,8 @@ _SIGNATURES = {
     "grn_surrogate_gradients": ([_P, _P, _P, _I, _P, ctypes.POINTER(_D)], _I),
     "grn_evolution_set_skip_clones": ([_P, _I], _I),
     "grn_evolution_set_surrogate": ([_P, _P, _D, _I, _I, _I, ctypes.c_float], _I),
+    "grn_evolution_set_surrogate_audit": ([_P, _I], _I),
+    "grn_evolution_set_surrogate_score": ([_P, _I], _I),
     "grn_evaluate_batch_noalloc": ([ctypes.POINTER(SimParams), _I, _P, _P,
                                     ctypes.POINTER(ModelBatchC), _P, _P, _P, _P,
                                     ctypes.c_char_p, _I], _I),
@@ -571,6 +576,15 @@ class Evolution:
         _check(self.lib.grn_evolution_set_surrogate(
             self.handle, surrogate.handle if surrogate else None, simulate_fraction,
             min_train_pairs, batches_per_generation, batch_size, lr))
+
+    def set_surrogate_score(self, score):
+        """grn_evolution_set_surrogate_score: SCORE_PARENT_ERROR or SCORE_PAIRED."""
+        _check(self.lib.grn_evolution_set_surrogate_score(self.handle, int(score)))
+
+    def set_surrogate_audit(self, enable=True):
+        """grn_evolution_set_surrogate_audit: also simulate rejected children
+        to measure the screen's recall (the search is unchanged)."""
+        _check(self.lib.grn_evolution_set_surrogate_audit(self.handle, 1 if enable else 0))
 
     def best(self):
         d, i = ctypes.c_int(), ctypes.c_int()

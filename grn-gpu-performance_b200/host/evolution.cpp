@@ -326,6 +326,7 @@ struct Individual {
   double parent_error = 1000;  // Individual.cpp:19-25: random individuals
   int complexity = 0;
   bool clone = false;  // same simulated program as its paired parent
+  const Individual *parent = nullptr;  // paired parent of a child (this generation)
 };
 
 struct Deme {
@@ -349,6 +350,8 @@ struct grn_evolution {
   void *user = nullptr;
   grn_ctx *ctx = nullptr;  // GPU evaluator (raw errors available), or null
   grn_surrogate *sur = nullptr;
+  bool sur_audit = false;  // also simulate the children the surrogate rejects
+  int sur_score = GRN_SCORE_PAIRED;  // grn_evolution_set_surrogate_score
   bool skip_clones = false;
   double sim_fraction = 0.25;
   int min_train = 2048, batches = 32, batch = 512;
@@ -471,6 +474,76 @@ grn_status feed_surrogate(grn_evolution *evo, const std::vector<Individual *> &i
     return grn_surrogate_train_batches(evo->sur, evo->batches, evo->batch, evo->lr,
                                        &st->surrogate_loss);
   return GRN_OK;
+}
+
+// Ranks with ties averaged (1-based), for Spearman's rank correlation.
+std::vector<double> average_ranks(const std::vector<double> &x) {
+  std::vector<int> o(x.size());
+  for (size_t i = 0; i < o.size(); ++i) o[i] = (int)i;
+  std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return x[a] < x[b]; });
+  std::vector<double> r(x.size());
+  for (size_t i = 0; i < o.size();) {
+    size_t j = i;
+    while (j + 1 < o.size() && x[o[j + 1]] == x[o[i]]) ++j;
+    for (size_t k = i; k <= j; ++k) r[o[k]] = 0.5 * (double)(i + j) + 1.0;
+    i = j + 1;
+  }
+  return r;
+}
+
+double spearman(const std::vector<double> &a, const std::vector<double> &b) {
+  if (a.size() < 3) return std::nan("");
+  const std::vector<double> ra = average_ranks(a), rb = average_ranks(b);
+  const double n = (double)a.size(), mean = (n + 1) / 2;
+  double sab = 0, saa = 0, sbb = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    sab += (ra[i] - mean) * (rb[i] - mean);
+    saa += (ra[i] - mean) * (ra[i] - mean);
+    sbb += (rb[i] - mean) * (rb[i] - mean);
+  }
+  return saa > 0 && sbb > 0 ? sab / std::sqrt(saa * sbb) : std::nan("");
+}
+
+// Quality of one generation's screen, from the simulated children: predicted
+// score (log error minus the parent's log error) against the simulated one.
+// rho over every simulated child; with an audit (every child simulated), the
+// recall of the screen: the share of the truly best k children (k = the
+// number it chose) that it chose, and the share of the children that beat
+// their parents that it chose.
+void screen_quality(const std::vector<Individual *> &todo, const std::vector<float> &pred,
+                    const std::vector<char> &chosen, const std::vector<double> &raw_all,
+                    const std::vector<char> &simulated, bool audited,
+                    grn_generation_stats *st) {
+  std::vector<double> p, a;
+  std::vector<int> idx;
+  for (size_t i = 0; i < todo.size(); ++i) {
+    if (!simulated[i]) continue;
+    const double r = raw_all[i];
+    if (!(r > 0) || !std::isfinite(r)) continue;
+    const double lp = std::log(std::max(todo[i]->parent_error, 1e-30));
+    p.push_back((double)pred[i] - lp);
+    a.push_back(std::log(r) - lp);
+    idx.push_back((int)i);
+  }
+  st->surrogate_rho = spearman(p, a);
+  st->surrogate_recall = std::nan("");
+  st->surrogate_improver_recall = std::nan("");
+  if (!audited || idx.empty()) return;
+  size_t k = 0;
+  for (char c : chosen) k += c != 0;
+  std::vector<int> o(idx.size());
+  for (size_t i = 0; i < o.size(); ++i) o[i] = (int)i;
+  std::stable_sort(o.begin(), o.end(), [&](int x, int y) { return a[x] < a[y]; });
+  size_t hit = 0, top = std::min(k, o.size());
+  for (size_t i = 0; i < top; ++i) hit += chosen[idx[o[i]]] != 0;
+  st->surrogate_recall = top ? (double)hit / (double)top : std::nan("");
+  size_t improvers = 0, kept = 0;
+  for (size_t i = 0; i < idx.size(); ++i)
+    if (raw_all[idx[i]] < todo[idx[i]]->parent_error) {
+      ++improvers;
+      kept += chosen[idx[i]] != 0;
+    }
+  st->surrogate_improver_recall = improvers ? (double)kept / (double)improvers : std::nan("");
 }
 
 void fill_stats(grn_evolution *evo, grn_generation_stats *st) {
@@ -792,6 +865,19 @@ grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
   return GRN_OK;
 }
 
+grn_status grn_evolution_set_surrogate_score(grn_evolution *evo, int score) {
+  if (!evo || (score != GRN_SCORE_PARENT_ERROR && score != GRN_SCORE_PAIRED))
+    return GRN_ERR_INVALID_ARGUMENT;
+  evo->sur_score = score;
+  return GRN_OK;
+}
+
+grn_status grn_evolution_set_surrogate_audit(grn_evolution *evo, int enable) {
+  if (!evo) return GRN_ERR_INVALID_ARGUMENT;
+  evo->sur_audit = enable != 0;
+  return GRN_OK;
+}
+
 grn_evolution::~grn_evolution() {
   if (primed) drain(this);
 }
@@ -845,12 +931,14 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
     for_each_deme(evo, [&](int d) {
       Deme &dm = evo->demes[d];
       reproduce(evo, dm);
+      for (size_t i = 0; i < dm.children.size(); ++i) dm.children[i].parent = &dm.pop[dm.perm[i]];
       if (!(evo->skip_clones || evo->sur)) return;
       // A child whose simulated program equals its paired parent's has the
       // parent's error: accept it without simulating (neutral drift kept).
       for (size_t i = 0; i < dm.children.size(); ++i) {
         Individual &c = dm.children[i];
         const Individual &p = dm.pop[dm.perm[i]];
+        c.parent = &p;
         c.clone = p.error < 100 && same_key(program_key(c.model, evo->ops.n_morph),
                                             program_key(p.model, evo->ops.n_morph));
         if (c.clone) c.error = p.error;
@@ -865,14 +953,37 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
   st.host_ms = ms_since(t0);
   // Surrogate screening: simulate only the most promising children.
   std::vector<Individual *> sim = todo;
-  if (evo->sur && evo->generation >= 0 &&
-      grn_surrogate_data_count(evo->sur) >= evo->min_train) {
+  std::vector<float> pred;
+  std::vector<char> chosen;
+  const bool screened = evo->sur && evo->generation >= 0 &&
+                        grn_surrogate_data_count(evo->sur) >= evo->min_train;
+  st.surrogate_rho = st.surrogate_recall = st.surrogate_improver_recall = std::nan("");
+  if (screened) {
     auto ts = std::chrono::steady_clock::now();
     FlatBatch fb(todo);
-    std::vector<float> feat((size_t)todo.size() * GRN_SURROGATE_FEATURES), pred(todo.size());
+    std::vector<float> feat((size_t)todo.size() * GRN_SURROGATE_FEATURES);
+    pred.assign(todo.size(), 0.0f);
     grn_status s = grn_encode_models(&fb.b, evo->ops.n_morph, feat.data());
     if (s == GRN_OK) s = grn_surrogate_predict(evo->sur, feat.data(), (int)todo.size(), pred.data());
     if (s != GRN_OK) return s;
+    if (evo->sur_score == GRN_SCORE_PAIRED) {
+      // Predicted change against the paired parent: the parent goes through
+      // the same network, so the error the network makes on a model family
+      // largely cancels between a child and its (near-copy) parent.  The
+      // score is shifted to the parent's true log error, so that it reads as
+      // a predicted log error.
+      std::vector<Individual *> parents(todo.size());
+      for (size_t i = 0; i < todo.size(); ++i)
+        parents[i] = const_cast<Individual *>(todo[i]->parent ? todo[i]->parent : todo[i]);
+      FlatBatch pb(parents);
+      std::vector<float> pf((size_t)todo.size() * GRN_SURROGATE_FEATURES), pp(todo.size());
+      s = grn_encode_models(&pb.b, evo->ops.n_morph, pf.data());
+      if (s == GRN_OK) s = grn_surrogate_predict(evo->sur, pf.data(), (int)todo.size(), pp.data());
+      if (s != GRN_OK) return s;
+      for (size_t i = 0; i < todo.size(); ++i)
+        pred[i] = (float)((double)pred[i] - pp[i] +
+                          std::log(std::max(todo[i]->parent_error, 1e-30)));
+    }
     std::vector<int> order(todo.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     auto score = [&](int i) {
@@ -880,12 +991,12 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score(a) < score(b); });
     const size_t n_sim = std::max<size_t>(1, (size_t)std::ceil(evo->sim_fraction * todo.size()));
-    sim.clear();
-    std::vector<char> chosen(todo.size(), 0);
+    chosen.assign(todo.size(), 0);
     for (size_t k = 0; k < n_sim && k < order.size(); ++k) chosen[order[k]] = 1;
-    for (size_t i = 0; i < todo.size(); ++i) {
-      if (chosen[i]) sim.push_back(todo[i]);
-      else todo[i]->error = HUGE_VAL;  // not simulated: its parent stays
+    if (!evo->sur_audit) {
+      sim.clear();
+      for (size_t i = 0; i < todo.size(); ++i)
+        if (chosen[i]) sim.push_back(todo[i]);
     }
     st.n_screened = (int32_t)todo.size();
     st.surrogate_ms += ms_since(ts);
@@ -897,6 +1008,34 @@ grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
   if (s != GRN_OK) {
     evo->last_error = "batch evaluation failed";
     return s;
+  }
+  if (screened) {
+    // Quality of the screen on what was simulated; then the rejected
+    // children lose to their parents (an audit's extra results only feed
+    // the statistics: the search and the training set are the unaudited
+    // run's).
+    std::vector<double> raw_all(todo.size(), std::nan(""));
+    std::vector<char> simulated(todo.size(), 0);
+    for (size_t i = 0, j = 0; i < todo.size(); ++i)
+      if (evo->sur_audit || chosen[i]) {
+        raw_all[i] = raw[j++];
+        simulated[i] = 1;
+      }
+    screen_quality(todo, pred, chosen, raw_all, simulated, evo->sur_audit, &st);
+    if (evo->sur_audit) {
+      std::vector<Individual *> kept;
+      std::vector<double> kept_raw;
+      for (size_t i = 0; i < todo.size(); ++i)
+        if (chosen[i]) {
+          kept.push_back(todo[i]);
+          kept_raw.push_back(raw_all[i]);
+        }
+      sim.swap(kept);
+      raw.swap(kept_raw);
+      st.n_audited = (int32_t)todo.size();
+    }
+    for (size_t i = 0; i < todo.size(); ++i)
+      if (!chosen[i]) todo[i]->error = HUGE_VAL;  // not simulated: its parent stays
   }
   if (evo->sur) {
     auto ts = std::chrono::steady_clock::now();

@@ -48,7 +48,7 @@
 extern "C" {
 #endif
 
-#define GRN_ABI_VERSION 1
+#define GRN_ABI_VERSION 2
 
 /* Capacity limits of the compiled model format.  A model whose products in
  * use or used links exceed these is rejected with GRN_ERR_CAPACITY. */
@@ -461,7 +461,17 @@ typedef struct grn_generation_stats {
   double surrogate_ms;       /* encode + predict + train, wall clock       */
   double surrogate_loss;     /* mean training loss of this generation      */
   int32_t n_clones;          /* children accepted without simulation       */
-  int32_t reserved0;
+  int32_t n_audited;         /* children simulated for the audit (else 0)  */
+  /* Quality of a surrogate screen (NaN without one): Spearman's rank
+   * correlation of the predicted and the simulated log(error) minus the
+   * parent's log(error), over the simulated children (all children under an
+   * audit, grn_evolution_set_surrogate_audit); under an audit also the share
+   * of the k truly best children that the screen chose (k = the number it
+   * chose), and the share of the children that beat their parents that it
+   * chose. */
+  double surrogate_rho;
+  double surrogate_recall;
+  double surrogate_improver_recall;
 } grn_generation_stats;
 
 /* A batch fitness evaluator: writes the rounded error (100 above
@@ -582,6 +592,24 @@ grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
 grn_status grn_evolution_set_surrogate(grn_evolution *evo, grn_surrogate *s,
                                        double simulate_fraction, int min_train_pairs,
                                        int batches_per_generation, int batch_size, float lr);
+
+/* How a screen ranks a child (grn_evolution_set_surrogate_score):
+ *   GRN_SCORE_PARENT_ERROR  predicted log(error) of the child minus the
+ *                           parent's simulated log(error);
+ *   GRN_SCORE_PAIRED        (default) predicted log(error) of the child
+ *                           minus the predicted log(error) of its paired
+ *                           parent, so that the network's bias on a model
+ *                           family cancels between a child and its parent. */
+#define GRN_SCORE_PARENT_ERROR 0
+#define GRN_SCORE_PAIRED 1
+grn_status grn_evolution_set_surrogate_score(grn_evolution *evo, int score);
+
+/* Audit of the surrogate screen: every screened generation also simulates
+ * the children the surrogate rejected, to measure the screen's recall
+ * (grn_generation_stats).  The search itself is unchanged -- rejected
+ * children still lose to their parents and train nothing -- so an audited
+ * run follows the unaudited run's trajectory at the full simulation cost. */
+grn_status grn_evolution_set_surrogate_audit(grn_evolution *evo, int enable);
 
 /* ------------------------------------------------ no-allocation entry ---
  * Device memory that grn_evaluate_batch_noalloc uses instead of allocating:

@@ -76,3 +76,46 @@ def island_shards(rank, world, port, root, out):
     evo.close()
     dist.barrier()
     dist.destroy_process_group()
+
+
+def cuda_one_rank(rank, world, port, root, out):
+    """ShardedEvaluator and IslandShards over the CUDA evaluator on a
+    one-rank NCCL process group (the same code paths a multi-GPU run takes:
+    deal, shard evaluation, all_gather; deme steps and the global-best
+    all_reduce)."""
+    for p in (os.path.join(root, "grn-gpu-performance_b200"), os.path.join(root, "oracle"),
+              os.path.join(root, "tests"), root):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import grn_b200 as grn
+    import sharded
+    import synth
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", 0))
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=41, n_models=37, steps=120)
+    me = np.full(batch.n_models, 1000.0)
+    me[::6] = 0.05
+    n_morph = params["n_input_morphogens"] + params["n_target_morphogens"]
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        err_s, raw_s, _ = sharded.ShardedEvaluator(ev, n_morph).evaluate_batch(batch, me)
+        err_p, raw_p, _ = ev.evaluate_batch(batch, me)
+        evo_p = dict(n_demes=4, deme_size=16, migration_period=2, n_max_products=6,
+                     n_max_links=10, n_host_threads=2, seed=5)
+        evo = grn.Evolution(evo_p, n_morph, evaluator=ev)
+        isl = sharded.IslandShards(evo, 4, 16, period=2, seed=3)
+        best_sharded = [isl.step()["global_best_error"] for _ in range(4)]
+        evo.close()
+        evo = grn.Evolution(evo_p, n_morph, evaluator=ev)
+        best_plain = [evo.step()["best_error"] for _ in range(4)]
+        evo.close()
+    np.savez(os.path.join(out, "rank%d.npz" % rank), err_s=err_s, raw_s=raw_s, err_p=err_p,
+             raw_p=raw_p, best_sharded=best_sharded, best_plain=best_plain)
+    dist.barrier()
+    dist.destroy_process_group()

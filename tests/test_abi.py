@@ -44,7 +44,7 @@ def test_library_exports_every_declared_symbol(built_libs):
 
 
 def test_abi_version(built_libs):
-    assert grn.load_library().grn_abi_version() == 1
+    assert grn.load_library().grn_abi_version() == 2
 
 
 @pytest.mark.skipif(__import__("conftest").HAS_GPU, reason="checks the no-device path")

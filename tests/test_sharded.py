@@ -73,3 +73,22 @@ def test_island_shards_migrate_across_ranks(built_libs, tmp_path):
                 mine["received"], other["sent"], got):
             assert np.array_equal(p1, p2) and np.array_equal(l1, l2) and err1 == err2
             assert np.array_equal(p3, p2) and np.array_equal(l3, l2) and err3 == err2
+
+
+@pytest.mark.gpu
+def test_sharding_runs_over_the_cuda_evaluator(built_libs, tmp_path):
+    """The sharding code over the real CUDA evaluator on a one-rank NCCL
+    group: the dealt-and-gathered errors equal a plain evaluate_batch bit for
+    bit and the FP64 oracle within the parity tolerance, and an island search
+    through IslandShards follows the plain search's trajectory."""
+    mp.spawn(dist_workers.cuda_one_rank, args=(1, _port(), ROOT, str(tmp_path)), nprocs=1,
+             join=True)
+    r = np.load(tmp_path / "rank0.npz")
+    np.testing.assert_array_equal(r["err_s"], r["err_p"])
+    np.testing.assert_array_equal(r["raw_s"], r["raw_p"])
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=41, n_models=37, steps=120)
+    me = np.full(batch.n_models, 1000.0)
+    me[::6] = 0.05
+    _, o_raw, _ = oracle.evaluate_batch(params, init, tgt, batch, me)
+    assert (np.abs(r["raw_s"] - o_raw) <= 1e-7 + 1e-4 * np.abs(o_raw)).all()
+    np.testing.assert_array_equal(r["best_sharded"], r["best_plain"])

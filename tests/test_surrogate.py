@@ -225,3 +225,60 @@ def test_evolution_with_surrogate_screening(built_libs):
         assert all(math.isfinite(s["surrogate_loss"]) for s in stats)
         evo.close()
         sur.close()
+
+
+def _search(ev, gens, seed, sur_seed=None, audit=False, score=None, fraction=0.25):
+    evo = grn.Evolution(dict(n_demes=8, deme_size=64, migration_period=5, n_max_products=6,
+                             n_max_links=12, n_host_threads=2, seed=seed), 2, evaluator=ev)
+    evo.set_skip_clones(True)
+    sur = None
+    if sur_seed is not None:
+        sur = grn.Surrogate(seed=sur_seed, capacity=20000)
+        evo.set_surrogate(sur, simulate_fraction=fraction, min_train_pairs=1024,
+                          batches_per_generation=16, batch_size=256)
+        if score is not None:
+            evo.set_surrogate_score(score)
+        if audit:
+            evo.set_surrogate_audit(True)
+    stats = [evo.step() for _ in range(gens)]
+    evo.close()
+    if sur:
+        sur.close()
+    return stats
+
+
+@pytest.mark.gpu
+def test_surrogate_screen_quality_against_no_network(built_libs):
+    """What the trained network gains over screening without it.  An audited
+    run (every child also simulated, the search unchanged) measures, per
+    screened generation, the share of the children that beat their parents
+    which the screen kept.  Without a network a screen keeping 25% of the
+    children keeps 25% of the improvers on average; the trained network's
+    screen must keep clearly more.  The audit must not change the search:
+    its trajectory equals the unaudited run's."""
+    params = dict(dim_x=16, dim_y=16, n_input_morphogens=1, n_target_morphogens=1,
+                  num_sim_steps=150, error_precision=8, fitness_kind=0, dt=0.1, min_conc=0.0,
+                  min_conc_change=0.0, dist_error_threshold=0.05)
+    wl = dict(synth.WORKLOADS["uneven_64x64"], W=16, H=16, n_exp=1)
+    init, tgt = synth.experiments(wl, 11)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        plain = _search(ev, 24, seed=7)
+        screened = _search(ev, 24, seed=7, sur_seed=3)
+        audited = _search(ev, 24, seed=7, sur_seed=3, audit=True)
+    assert [s["best_error"] for s in audited] == [s["best_error"] for s in screened]
+    assert [s["n_evaluated"] for s in audited] == [s["n_evaluated"] for s in screened]
+    rows = [s for s in audited if s["n_screened"]]
+    assert len(rows) >= 10
+    assert all(s["n_audited"] == s["n_screened"] for s in rows)
+    rec = np.array([s["surrogate_improver_recall"] for s in rows], np.float64)
+    rho = np.array([s["surrogate_rho"] for s in rows], np.float64)
+    rec, rho = rec[np.isfinite(rec)], rho[np.isfinite(rho)]
+    print("improver recall %.3f (no network: 0.25), rho %.3f, best plain %.5f screened %.5f, "
+          "simulations plain %d screened %d" % (
+              rec.mean(), rho.mean(), plain[-1]["best_error"], screened[-1]["best_error"],
+              sum(s["n_evaluated"] for s in plain), sum(s["n_evaluated"] for s in screened)))
+    assert len(rec) >= 5 and rec.mean() >= 0.35
+    assert rho.mean() > 0.1
+    # The screened search simulates far fewer children than the plain one.
+    assert sum(s["n_evaluated"] for s in screened) < 0.6 * sum(s["n_evaluated"] for s in plain)
