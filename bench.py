@@ -413,7 +413,8 @@ def main():
     ap.add_argument("--euler-steps", type=int, default=None,
                     help="override the workload's Euler step count (small profiling cases)")
     ap.add_argument("--schedule", default="auto",
-                    choices=["auto", "fixed_items", "walk_items", "global", "cluster", "stream"],
+                    choices=["auto", "fixed_items", "walk_items", "global", "cluster", "stream",
+                             "stream2"],
                     help="force a kernel schedule instead of the autotuner's choice")
     ap.add_argument("--pipeline", action="store_true",
                     help="island workloads: two deme halves alternate on the GPU while the "

@@ -64,7 +64,8 @@ struct KernelVariant {
   bool cluster; // cluster-split: a cluster of CTAs per model, one band of
                 // rows each
   bool trace;   // writes trace frames (SimArgs::trace_out)
-  bool stream;  // streaming schedule (SimArgs::band_rows)
+  int stream;   // 0; 1 streaming schedule (SimArgs::band_rows); 2 streaming
+                // with two Euler steps per pass (temporal blocking)
 };
 
 // Launch plan chosen by the host.

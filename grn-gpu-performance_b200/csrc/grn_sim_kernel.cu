@@ -814,10 +814,12 @@ __device__ __forceinline__ void group_step_fast(const ModelSmem &M, const DenseS
 
 // New values of all genes of NI groups of one band (stage planes of
 // gb.PS floats), written to the global next-state planes.
+// `out` addresses the band's cells as a plane does: cell (x, local row y)
+// of gene p at out + p * gps + (y + 1) * RS + x.
 template <int NI, int GS, bool EXACT, bool RAGGED>
 __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseSmem &D,
                                                 const float *stage, int G, const Geom &gb,
-                                                const Item (&it)[NI], float *gl_nxt, size_t gps,
+                                                const Item (&it)[NI], float *out, size_t gps,
                                                 float dt, float min_conc, float &mx) {
   const uint32_t lg_mask = M.hdr.lg_mask;
   float4 lg[NI][GS];
@@ -839,8 +841,6 @@ __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseS
       }
     }
   }
-  // stage row 0 is plane row gb.y0 (grid row gb.y0 - 1)
-  float *out = gl_nxt + (size_t)gb.y0 * gb.RS;
   for (int p = 0; p < G; ++p) {
     float4 nv[NI];
     gene_update<NI, GS, EXACT, RAGGED>(M, D, p, M.genes[p], lg, stage + p * gb.PS, gb, it, dt,
@@ -855,22 +855,22 @@ template <int NI, int GMAX, bool RAGGED>
 __device__ __forceinline__ void band_group_step_any(bool exact, const ModelSmem &M,
                                                     const DenseSmem &D, const float *stage, int G,
                                                     const Geom &gb, const Item (&it)[NI],
-                                                    float *gl_nxt, size_t gps, float dt,
+                                                    float *out, size_t gps, float dt,
                                                     float min_conc, float &mx) {
   if (exact)
-    band_group_step<NI, GMAX, true, RAGGED>(M, D, stage, G, gb, it, gl_nxt, gps, dt, min_conc,
+    band_group_step<NI, GMAX, true, RAGGED>(M, D, stage, G, gb, it, out, gps, dt, min_conc,
                                             mx);
   else if (GMAX > 2 && G <= 2)
-    band_group_step<NI, (GMAX < 2 ? GMAX : 2), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+    band_group_step<NI, (GMAX < 2 ? GMAX : 2), false, RAGGED>(M, D, stage, G, gb, it, out,
                                                               gps, dt, min_conc, mx);
   else if (GMAX > 4 && G <= 4)
-    band_group_step<NI, (GMAX < 4 ? GMAX : 4), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+    band_group_step<NI, (GMAX < 4 ? GMAX : 4), false, RAGGED>(M, D, stage, G, gb, it, out,
                                                               gps, dt, min_conc, mx);
   else if (GMAX > 6 && G <= 6)
-    band_group_step<NI, (GMAX < 6 ? GMAX : 6), false, RAGGED>(M, D, stage, G, gb, it, gl_nxt,
+    band_group_step<NI, (GMAX < 6 ? GMAX : 6), false, RAGGED>(M, D, stage, G, gb, it, out,
                                                               gps, dt, min_conc, mx);
   else
-    band_group_step<NI, GMAX, false, RAGGED>(M, D, stage, G, gb, it, gl_nxt, gps, dt, min_conc,
+    band_group_step<NI, GMAX, false, RAGGED>(M, D, stage, G, gb, it, out, gps, dt, min_conc,
                                              mx);
 }
 
@@ -887,8 +887,7 @@ template <int NT, int GMAX, bool RAGGED>
 __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSmem &D,
                             const StatePtrs &sp, const Geom &g, int G, int par, bool exact,
                             float dt, float min_conc, float &mx, uint64_t *bars,
-                            uint32_t &mphase, volatile int *fail) {
-  const int R = A.band_rows;
+                            uint32_t &mphase, volatile int *fail, int R) {
   const int nb = (g.H + R - 1) / R;
   const int SPS = (R + 2) * g.RS;
   float *stage0 = sp.sm;
@@ -927,8 +926,9 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     const int n_it = (gb.Q + NT - 1) / NT;
     for (int i = 0; i < n_it; ++i) {  // the same count in every thread (barriers follow)
       const Item it[1] = {item_at(threadIdx.x + i * NT, gb)};
-      band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st, G, gb, it, gl_nxt, gps, dt,
-                                            min_conc, mx);
+      band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st, G, gb, it,
+                                            gl_nxt + (size_t)gb.y0 * g.RS, gps, dt, min_conc,
+                                            mx);
     }
     __syncthreads();  // stage s is free again; *fail is the same for every thread
     if (*fail) {
@@ -941,6 +941,113 @@ __device__ bool stream_step(const SimArgs &A, const ModelSmem &M, const DenseSme
     if (threadIdx.x == 0 && b + 2 < nb) issue(b + 2);
   }
   fence_proxy_async_global();  // this step's writes before the next step's copies
+  return true;
+}
+
+// ---- temporal blocking: two Euler steps per pass over the state --------
+//
+// The streaming schedule reads and writes every plane once per step.  This
+// variant (kernel ST == 2) advances the state two steps per pass.  A band
+// of R output rows (grid rows [bR, bR + R)) needs the current state of
+// grid rows [bR - 2, bR + R + 2): plane rows [bR - 1, bR + R + 3), clipped
+// to the plane, arrive in one shared-memory stage by bulk copies.  Step one
+// computes grid rows [bR - 1, bR + R] (clipped to the grid) from the stage
+// into an intermediate buffer of R + 2 rows -- the band and one halo row on
+// either side, which the neighbouring bands compute as well; step two
+// computes the band from the intermediate and writes it to the global
+// next-state planes.  The copy of band b + 1 is issued once step one of band
+// b has read the stage, so it overlaps step two.  Both steps run
+// band_group_step, the one-step schedules' arithmetic, so states are
+// bit-identical to them.  Shared memory: G * (R + 4) stage rows and
+// G * (R + 2) intermediate rows (R = A.band_rows); the same space holds the
+// one-step schedule's two stages of R + 1 + 2 rows, which the kernel uses
+// for a single step (an odd last step, or a first step after which the
+// simulation stops).
+//
+// mx1 / mx2 receive the threads' max |rate| of the first / second step.
+// Returns false (the same in every thread) if a copy did not complete in
+// time, after a bounded wait for the copy still in flight.
+template <int NT, int GMAX, bool RAGGED>
+__device__ bool stream_step2(const SimArgs &A, const ModelSmem &M, const DenseSmem &D,
+                             const StatePtrs &sp, const Geom &g, int G, int par, bool exact,
+                             float dt, float min_conc, float &mx1, float &mx2, uint64_t *bars,
+                             uint32_t &mphase, volatile int *fail) {
+  const int R = A.band_rows;
+  const int nb = (g.H + R - 1) / R;
+  const int SPS = (R + 4) * g.RS;   // stage plane stride: plane rows bR-1 .. bR+R+2
+  const int IPS = (R + 2) * g.RS;   // intermediate plane stride: grid rows bR-1 .. bR+R
+  float *stage = sp.sm;
+  float *inter = sp.sm + (size_t)GMAX * SPS;
+  const size_t gps = (size_t)g.PS;
+  const float *gl_cur = sp.gl + (par ? GMAX : 0) * gps;
+  float *gl_nxt = sp.gl + (par ? 0 : GMAX) * gps;
+  auto issue = [&](int b) {
+    const int p0 = max(b * R - 1, 0);               // first plane row copied
+    const int p1 = min(b * R + R + 3, g.H + 2);     // one past the last
+    const int off = p0 - (b * R - 1);               // its stage row (1 for band 0)
+    const uint32_t bytes = (uint32_t)(p1 - p0) * g.RS * 4u;
+    fence_proxy_async_shared();
+    mbar_expect_tx(bars, bytes * (uint32_t)G);
+    for (int p = 0; p < G; ++p) {
+      float *dst = stage + p * SPS + off * g.RS;
+      const float *src = gl_cur + p * gps + (size_t)p0 * g.RS;
+      if (chk_copy(dst, src, (long)(p1 - p0) * g.RS)) bulk_g2s(dst, src, bytes, bars);
+    }
+  };
+  if (threadIdx.x == 0) issue(0);
+  for (int b = 0; b < nb; ++b) {
+    const uint32_t parity = mphase & 1u;
+    if (!mbar_wait(bars, parity)) *fail = 1;
+    mphase ^= 1u;
+    // Step one: grid rows [y1, y1 + h1) into the intermediate.
+    const int y1 = max(b * R - 1, 0);
+    const int h1 = min(b * R + R, g.H - 1) - y1 + 1;
+    Geom g1 = g;
+    g1.y0 = y1;
+    g1.H = h1;
+    g1.PS = SPS;
+    g1.Q = h1 * g.Wg;
+    // Stage row of grid row y is y - bR + 2; g1's row 0 is grid row y1 - 1.
+    const float *st1 = stage + (y1 - b * R + 1) * g.RS;
+    float *out1 = inter + (y1 - b * R) * g.RS;  // cell rows land at y - (bR - 1)
+    const int n1 = (g1.Q + NT - 1) / NT;
+    for (int i = 0; i < n1; ++i) {
+      const Item it[1] = {item_at(threadIdx.x + i * NT, g1)};
+      band_group_step_any<1, GMAX, RAGGED>(exact, M, D, st1, G, g1, it, out1, (size_t)IPS, dt,
+                                            min_conc, mx1);
+    }
+    // Intermediate rows outside the grid are the planes' zero rows.
+    const int zlo = (b == 0) ? 0 : -1;                            // grid row -1
+    const int zhi = (b * R + R >= g.H) ? g.H - (b * R - 1) : -1;  // grid row H
+    for (int i = threadIdx.x; i < 2 * G * g.RS; i += NT) {
+      const int z = i / (G * g.RS), r = i - z * G * g.RS;
+      const int row = z == 0 ? zlo : zhi;
+      if (row < 0) continue;
+      const int p = r / g.RS, x = r - p * g.RS;
+      *chk<1>(inter + p * IPS + row * g.RS + x) = 0.0f;
+    }
+    __syncthreads();  // the stage is free; the intermediate is complete
+    if (*fail) {
+      mbar_wait(bars, parity);  // bounded second wait for the copy still in flight
+      return false;
+    }
+    if (threadIdx.x == 0 && b + 1 < nb) issue(b + 1);
+    // Step two: the band's rows from the intermediate.
+    Geom g2 = g;
+    g2.y0 = b * R;
+    g2.H = min(R, g.H - b * R);
+    g2.PS = IPS;
+    g2.Q = g2.H * g.Wg;
+    const int n2 = (g2.Q + NT - 1) / NT;
+    for (int i = 0; i < n2; ++i) {
+      const Item it[1] = {item_at(threadIdx.x + i * NT, g2)};
+      band_group_step_any<1, GMAX, RAGGED>(exact, M, D, inter, G, g2, it,
+                                            gl_nxt + (size_t)g2.y0 * g.RS, gps, dt, min_conc,
+                                            mx2);
+    }
+    __syncthreads();  // the intermediate is free again
+  }
+  fence_proxy_async_global();  // this pass's writes before the next pass's copies
   return true;
 }
 
@@ -1013,7 +1120,7 @@ __device__ __forceinline__ void cluster_share(T *slots, T v, int rank, int C) {
 //           and passes the same cluster barriers: the model index, the step
 //           max and the fitness sum are shared values, identical bits in
 //           every CTA.
-template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL, bool TRACE, bool ST>
+template <int NT, int GMAX, int ITEMS, bool LOOP, bool RAGGED, bool CL, bool TRACE, int ST>
 __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   ModelSmem &M = *reinterpret_cast<ModelSmem *>(smem);
@@ -1188,9 +1295,43 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
       int par = 0;  // buffer holding the current values
       while (step < A.n_steps && change > A.min_conc_change) {
         float mx = 0.0f;
-        if constexpr (ST) {
+        int adv = 1;  // Euler steps this iteration advanced
+        if constexpr (ST == 2) {
+          // Two steps per pass while two remain.  If the first step's change
+          // already ends the simulation, that step is run alone again (the
+          // one-step pass, R + 1 rows per band in the same shared memory),
+          // so the state is the one after exactly one step.
+          bool ok;
+          if (step + 2 <= A.n_steps) {
+            float mx2 = 0.0f;
+            ok = stream_step2<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
+                                                mx2, bars, mphase, s_stream_fail);
+            if (ok) {
+              const float b1 = block_max<NT>(mx, s_red, par ^ 1, lane, warp);
+              if ((double)b1 > A.min_conc_change) {
+                mx = mx2;
+                adv = 2;
+              } else {
+                mx = 0.0f;
+                ok = stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc,
+                                                   mx, bars, mphase, s_stream_fail,
+                                                   A.band_rows + 1);
+              }
+            }
+          } else {
+            ok = stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
+                                               bars, mphase, s_stream_fail, A.band_rows + 1);
+          }
+          if (!ok) {
+            if (tid == 0) {
+              atomicExch(A.error_flag, 2);
+              A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
+            }
+            return;  // every thread of the block: the decision is block-uniform
+          }
+        } else if constexpr (ST) {
           if (!stream_step<NT, GMAX, RAGGED>(A, M, D, sp, g, G, par, exact, dt, min_conc, mx,
-                                              bars, mphase, s_stream_fail)) {
+                                              bars, mphase, s_stream_fail, A.band_rows)) {
             if (tid == 0) {
               atomicExch(A.error_flag, 2);
               A.raw_error[orig] = __longlong_as_double(0x7ff8000000000000ll);
@@ -1246,7 +1387,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         }
         change = (double)bm;
         par ^= 1;
-        ++step;
+        step += adv;
         if constexpr (TRACE) {
           if (step % A.trace_every == 0 && step / A.trace_every < A.trace_frames)
             write_planes<NT, GMAX>(A, sp, g, G, par,
@@ -1314,7 +1455,7 @@ struct VariantEntry {
    &sim_kernel<NT, GMAX, ITEMS, LOOP, false, CL, TR, ST>},                                \
   {{NT, GMAX, ITEMS, LOOP, true, CL, TR, ST}, &sim_kernel<NT, GMAX, ITEMS, LOOP, true, CL, TR, ST>}
 #define GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, TR) \
-  GRN_VARIANT_X(NT, GMAX, ITEMS, LOOP, CL, TR, false)
+  GRN_VARIANT_X(NT, GMAX, ITEMS, LOOP, CL, TR, 0)
 #define GRN_VARIANT(NT, GMAX, ITEMS, LOOP, CL) GRN_VARIANT_T(NT, GMAX, ITEMS, LOOP, CL, false)
 
 const VariantEntry kVariants[] = {
@@ -1329,8 +1470,11 @@ const VariantEntry kVariants[] = {
     // trace frames (one model at a time: any grid, any gene count)
     GRN_VARIANT_T(256, 16, 1, true, false, true),
     // streaming (bands staged by bulk copies)
-    GRN_VARIANT_X(512, 8, 1, true, false, false, true),
-    GRN_VARIANT_X(512, 16, 1, true, false, false, true),
+    GRN_VARIANT_X(512, 8, 1, true, false, false, 1),
+    GRN_VARIANT_X(512, 16, 1, true, false, false, 1),
+    // streaming with temporal blocking: two Euler steps per pass
+    GRN_VARIANT_X(512, 8, 1, true, false, false, 2),
+    GRN_VARIANT_X(512, 16, 1, true, false, false, 2),
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 

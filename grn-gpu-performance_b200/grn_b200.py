@@ -31,12 +31,13 @@ FITNESS_MSE = 1
 SCHEDULE_AUTO, SCHEDULE_FIXED_ITEMS, SCHEDULE_WALK_ITEMS, SCHEDULE_GLOBAL = 0, 1, 2, 3
 SCHEDULE_CLUSTER = 4
 SCHEDULE_STREAM = 5
+SCHEDULE_STREAM2 = 6
 TEST_WITHHOLD_BAND_COPY = 1
 TEST_FAIL_DEVICE_ALLOC = 2
 TEST_CORRUPT_RECORD = 4
 SCORE_PARENT_ERROR, SCORE_PAIRED = 0, 1
 SCHEDULE_NAMES = {0: "auto", 1: "fixed_items", 2: "walk_items", 3: "global", 4: "cluster",
-                  5: "stream"}
+                  5: "stream", 6: "stream2"}
 
 
 class SimParams(ctypes.Structure):

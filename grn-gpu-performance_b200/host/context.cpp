@@ -230,6 +230,26 @@ int stream_rows(int W, int H, int gmax, size_t room, int threads) {
   return (int)r;
 }
 
+// Output rows per band of the two-steps-per-pass streaming variant: its
+// stage holds R + 4 rows of every gene and its intermediate R + 2, i.e.
+// gmax * (2R + 6) rows (the one-step pass it falls back to uses the same
+// space as two stages of R + 3 rows).  Rows of a pass's step one are a
+// multiple of the block's threads where that is possible.
+int stream2_rows(int W, int H, int gmax, size_t room, int threads) {
+  const int Wg = (W + 3) / 4;
+  const size_t row_bytes = (size_t)grn::row_floats(W) * sizeof(float);
+  long r = ((long)(room / (gmax * row_bytes)) - 6) / 2;
+  r = std::min<long>(r, H);
+  // One pass's copies complete on one mbarrier (transaction count < 2^20).
+  while (r > 1 && (size_t)gmax * (r + 4) * row_bytes >= (size_t)1 << 20) --r;
+  if (r < 1) return 0;
+  if (threads % Wg == 0) {
+    const long per = threads / Wg;  // rows per full pass of the block's threads
+    if (r + 2 >= per && (r + 2) % per != 0) r -= (r + 2) % per;
+  }
+  return r >= 1 ? (int)r : 0;
+}
+
 grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace,
                            std::vector<std::pair<double, LaunchPlan>> *out) {
   const int W = ctx->p.dim_x, H = ctx->p.dim_y;
@@ -248,21 +268,25 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace
     if (ctx->forced_threads && !trace && v.threads != ctx->forced_threads) continue;
     if (v.stream) {
       // Streaming: only where the planes do not all fit shared memory.
-      if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_STREAM) continue;
+      const int own = v.stream == 2 ? GRN_SCHEDULE_STREAM2 : GRN_SCHEDULE_STREAM;
+      if (sched != GRN_SCHEDULE_AUTO && sched != own) continue;
       const size_t plane_bytes = (size_t)grn::plane_floats(W, H) * sizeof(float);
       const int fit = optin > fixed ? (int)((optin - fixed) / plane_bytes) & ~1 : 0;
       if (sched == GRN_SCHEDULE_AUTO && fit / 2 >= max_genes) continue;
-      const int R = stream_rows(W, H, v.gmax, optin > fixed ? optin - fixed : 0, v.threads);
+      const size_t room = optin > fixed ? optin - fixed : 0;
+      const int R = v.stream == 2 ? stream2_rows(W, H, v.gmax, room, v.threads)
+                                  : stream_rows(W, H, v.gmax, room, v.threads);
       if (R < 1) continue;
-      const size_t smem =
-          fixed + (size_t)2 * v.gmax * (R + 2) * grn::row_floats(W) * sizeof(float);
+      const size_t rows = v.stream == 2 ? (size_t)v.gmax * (2 * R + 6)
+                                        : (size_t)2 * v.gmax * (R + 2);
+      const size_t smem = fixed + rows * grn::row_floats(W) * sizeof(float);
       int per_sm = 0;
       GRN_CUDA(ctx, grn::sim_occupancy(v, smem, &per_sm));
       const int ctas = per_sm * ctx->n_sm;
       if (ctas < 1) continue;
       LaunchPlan plan{};
       plan.v = v;
-      plan.schedule = GRN_SCHEDULE_STREAM;
+      plan.schedule = own;
       plan.planes = 0;
       plan.smem_bytes = smem;
       plan.blocks_per_sm = per_sm;
@@ -276,7 +300,7 @@ grn_status enumerate_plans(grn_ctx *ctx, int max_genes, int n_models, bool trace
       out->push_back({busy * 0.6 - 1e-3 * v.gmax, plan});
       continue;
     }
-    if (sched == GRN_SCHEDULE_STREAM) continue;
+    if (sched == GRN_SCHEDULE_STREAM || sched == GRN_SCHEDULE_STREAM2) continue;
     if (sched == GRN_SCHEDULE_CLUSTER && !v.cluster) continue;
     if (sched != GRN_SCHEDULE_AUTO && sched != GRN_SCHEDULE_CLUSTER && v.cluster) continue;
     if (sched == GRN_SCHEDULE_FIXED_ITEMS && v.loop) continue;
@@ -919,7 +943,7 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size) {
 
 grn_status grn_set_schedule(grn_ctx *ctx, int schedule, int threads_per_block) {
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
-  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_STREAM || threads_per_block < 0)
+  if (schedule < GRN_SCHEDULE_AUTO || schedule > GRN_SCHEDULE_STREAM2 || threads_per_block < 0)
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "bad schedule");
   ctx->forced_schedule = schedule;
   ctx->forced_threads = threads_per_block;

@@ -130,10 +130,23 @@ grn_status pack_model(const grn_product *products, int n_products,
         pl.a = 0.0f;
         pl.b = 0.0f;
       } else {
-        const double lk2 = std::log2(lk->dis_const);
+        // lg2 of the reference's K^n = pow(K, n) (simophillact.cpp:9-12):
+        // n * lg2(K) for a positive K; for K <= 0 lg2 of pow(K, n) itself
+        // (positive for an even integer n, NaN -- as the reference's Hill
+        // value then is for every x -- for a negative or NaN power).  A K^n
+        // of 0 is -inf, so that x = 0 gives the reference's 0/0 = NaN; a
+        // repression K^n that overflows is NaN (the reference's inf/inf).
+        // A negative K^n (odd integer n) makes the Hill term x^n/(x^n + K^n)
+        // non-monotone, which exponent form cannot hold: its term is NaN.
+        const double kn = std::pow(lk->dis_const, n);
+        double lk2;
+        if (kn == 0) lk2 = -HUGE_VAL;
+        else if (lk->dis_const > 0) lk2 = n * std::log2(lk->dis_const);
+        else lk2 = kn > 0 ? std::log2(kn) : std::nan("");
+        if (!act && kn == HUGE_VAL) lk2 = std::nan("");
         pl.slot = index_of(lk->regulator);
         pl.a = (float)(act ? -n : n);
-        pl.b = (float)(act ? n * lk2 : -n * lk2);
+        pl.b = (float)(act ? lk2 : -lk2);
         hdr.lg_mask |= 1u << pl.slot;
       }
       plinks.push_back(pl);

@@ -165,10 +165,15 @@ typedef enum grn_schedule {
                                    per model, each CTA a band of rows in
                                    its shared memory, halo rows exchanged
                                    through distributed shared memory      */
-  GRN_SCHEDULE_STREAM = 5       /* every plane in global memory; each step
+  GRN_SCHEDULE_STREAM = 5,      /* every plane in global memory; each step
                                    walks bands of rows staged through
                                    shared memory by bulk (TMA) copies,
                                    double-buffered                        */
+  GRN_SCHEDULE_STREAM2 = 6      /* as GRN_SCHEDULE_STREAM with temporal
+                                   blocking: each pass over the planes
+                                   advances two Euler steps (half the
+                                   state traffic; step one recomputes one
+                                   halo row per band side)                */
 } grn_schedule;
 
 typedef struct grn_ctx grn_ctx;

@@ -72,6 +72,7 @@ def run_cases():
                                                   links=(1, 24), n_exp=2)
         batch.links["dis_const"][0] = 0.0
         _states(out, "stream%dx%d" % (W, H), params, batch, init, tgt, grn.SCHEDULE_STREAM)
+        _states(out, "stream2_%dx%d" % (W, H), params, batch, init, tgt, grn.SCHEDULE_STREAM2)
     # Cluster-split: halo rows through distributed shared memory and, at
     # 256 x 256, through neighbouring blocks' global slots.
     params, batch, init, tgt = synth.workload("uneven_64x64", seed=6, n_models=8, steps=20,

@@ -298,6 +298,52 @@ def test_stream_schedule_early_exit_bitwise():
     assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream early exit")
 
 
+@pytest.mark.parametrize("W,H,steps,genes", [(256, 256, 12, (8, 8)), (100, 100, 31, (6, 8)),
+                                             (30, 37, 25, (2, 8)), (250, 90, 15, (8, 16)),
+                                             (64, 5, 9, (2, 6))])
+def test_stream2_schedule_matches_global_bitwise(W, H, steps, genes):
+    """Temporal blocking (two Euler steps per pass, GRN_SCHEDULE_STREAM2):
+    the same per-cell arithmetic as the all-global schedule, identical
+    states, including an odd step count (the last step alone), ragged
+    widths, a last band shorter than the others, a grid of one band,
+    16-gene models and the exact path."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=23, n_models=12, steps=steps,
+                                              W=W, H=H, genes=genes, links=(1, 24), n_exp=2)
+    batch.links["dis_const"][0] = 0.0  # model 0 takes the exact path
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=16)
+        ev.set_schedule(grn.SCHEDULE_STREAM2)
+        raw, states = ev.evaluate_states(batch, max_planes=16)
+        _, raw_b, st = ev.evaluate_batch(batch)
+    assert st["schedule"] == grn.SCHEDULE_STREAM2
+    assert np.array_equal(states, base_states)
+    assert np.array_equal(raw, raw_b)
+    assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream2")
+
+
+def test_stream2_early_exit_bitwise():
+    """Early exit under temporal blocking: where the change after the first
+    step of a pass ends the simulation, that step is redone alone, so final
+    states and step counts match the all-global schedule."""
+    params, batch, init, tgt = synth.workload("small_32x32", seed=25, n_models=24, steps=3000,
+                                              W=40, H=36, min_conc_change=1e-2, fitness=0,
+                                              n_exp=2)
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_schedule(grn.SCHEDULE_GLOBAL)
+        base_raw, base_states = ev.evaluate_states(batch, max_planes=8)
+        _, _, base_st = ev.evaluate_batch(batch)
+        ev.set_schedule(grn.SCHEDULE_STREAM2)
+        raw, states = ev.evaluate_states(batch, max_planes=8)
+        _, _, st = ev.evaluate_batch(batch)
+    assert st["schedule"] == grn.SCHEDULE_STREAM2
+    assert st["total_steps"] == base_st["total_steps"] < 24 * 2 * 3000
+    assert np.array_equal(states, base_states)
+    assert_raw_close(raw, base_raw, rtol=1e-12, atol=0, what="stream2 early exit")
+
+
 def test_stream_copy_wait_times_out_cleanly():
     """A bulk copy that never arrives (test hook): the kernel's bounded wait
     runs out after about a second, the call reports it, and the context
