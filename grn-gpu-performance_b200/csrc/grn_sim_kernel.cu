@@ -1276,6 +1276,14 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
         float *pl = plane_of<GMAX>(sp, g, kk, kb < G ? 0 : 1);
         *chk<1>(pl + r) = v;
       }
+      if constexpr (ST == 2) {
+        // The two-step pass's intermediate buffer: its rows' trailing zero
+        // cells are never written by a step, so they start at 0 here (the
+        // one-step pass's stage copies that may land there carry the
+        // planes' zero cells in the same columns).
+        float *inter = sp.sm + (size_t)GMAX * (A.band_rows + 4) * g.RS;
+        for (int i = tid; i < GMAX * (A.band_rows + 2) * g.RS; i += NT) *chk<1>(inter + i) = 0.0f;
+      }
       if constexpr (ST) fence_proxy_async_global();  // before the first bulk copies
       if constexpr (CL) cg::this_cluster().sync();
       else __syncthreads();

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in tests/golden/.
 
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py [--reference DIR]
 
 reference_test_model.json
     The reference's only known-answer fixture: the test-model string of
@@ -33,11 +33,19 @@ import pyoracle  # noqa: E402
 import synth  # noqa: E402
 from grn_b200 import ModelBatch  # noqa: E402
 
-REF_SRC = "/root/reference/Src/UI/Evolution/errorcalculatormultithread.cpp"
+REF_FILE = os.path.join("Src", "UI", "Evolution", "errorcalculatormultithread.cpp")
 
 
-def reference_test_model():
-    with open(REF_SRC) as f:
+def reference_source(root):
+    """The reference file holding its test model, under the checkout `root`
+    (the --reference argument, else $GRN_REFERENCE_ROOT, else
+    /root/reference)."""
+    root = root or os.environ.get("GRN_REFERENCE_ROOT", "/root/reference")
+    return os.path.join(root, REF_FILE)
+
+
+def reference_test_model(path):
+    with open(path) as f:
         lines = f.read().splitlines()
     model = re.search(r'QString modelStr\("(.*)"\);', lines[60]).group(1)
     expected = re.search(r"double expectedError = ([0-9.eE+-]+);", lines[61]).group(1)
@@ -97,9 +105,13 @@ def small_cases():
 
 
 def main():
-    if os.path.exists(REF_SRC):
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=None, help="reference checkout")
+    src = reference_source(ap.parse_args().reference)
+    if os.path.exists(src):
         with open(os.path.join(HERE, "reference_test_model.json"), "w") as f:
-            json.dump(reference_test_model(), f, indent=1)
+            json.dump(reference_test_model(src), f, indent=1)
     with open(os.path.join(HERE, "oracle_small.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "cases": small_cases()}, f)
     print("fixtures written")
