@@ -614,11 +614,10 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
         // Row borders read the zero cells that end every padded row.
         const float lft = *chk<1>(cur + it[i].base - 1);
         const float rgt = *chk<1>(cur + it[i].base + 4);
-        // Reference order: x-1, x+1, y-1, y+1.
-        const float2 s01 = add2(add2(add2(make_float2(lft, c.x), make_float2(c.y, c.z)),
-                                     lo2(up)), lo2(dn));
-        const float2 s23 = add2(add2(add2(make_float2(c.y, c.z), make_float2(c.w, rgt)),
-                                     hi2(up)), hi2(dn));
+        // Reference order: x-1, x+1, y-1, y+1.  The horizontal pairs are
+        // scalar adds (their operands straddle the float4's register pairs).
+        const float2 s01 = add2(add2(make_float2(lft + c.y, c.x + c.z), lo2(up)), lo2(dn));
+        const float2 s23 = add2(add2(make_float2(c.y + c.w, c.z + rgt), hi2(up)), hi2(dn));
         r01 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.x, -it[i].tot.y), lo2(c), s01), r01);
         r23 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.z, -it[i].tot.w), hi2(c), s23), r23);
       }
@@ -626,7 +625,7 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
       const float2 n23 = fma2(f2(dt), r23, hi2(c));
       nv[i] = make_float4(fmaxf(n01.x, 0.0f), fmaxf(n01.y, 0.0f), fmaxf(n23.x, 0.0f),
                           fmaxf(n23.y, 0.0f));
-      float m = fmaxf(fabsf(r01.x), 0.0f);
+      float m = fabsf(r01.x);
       float m1 = fabsf(r01.y), m2 = fabsf(r23.x), m3 = fabsf(r23.y);
       if constexpr (RAGGED) {
         // Cells past W are padding: kept at 0, never part of the max.
@@ -634,8 +633,7 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
         if (!it[i].v2) { nv[i].z = 0.0f; m2 = 0.0f; }
         if (!it[i].v3) { nv[i].w = 0.0f; m3 = 0.0f; }
       }
-      m = fmaxf(fmaxf(m, m1), fmaxf(m2, m3));
-      if (it[i].valid) mx = fmaxf(mx, m);
+      if (it[i].valid) mx = fmaxf(fmaxf(mx, m), fmaxf(fmaxf(m1, m2), m3));
     }
     return;
   }
@@ -684,13 +682,9 @@ __device__ __forceinline__ float block_max(float v, float *red, int parity, int 
   float *r = red + parity * 32;
   if (lane == 0) r[warp] = __uint_as_float(bits);
   __syncthreads();
-  float m = 0.0f;
-#pragma unroll
-  for (int w = 0; w < NT / 32; w += 4) {
-    const float4 v4 = *reinterpret_cast<const float4 *>(r + w);
-    m = fmaxf(m, fmaxf(fmaxf(v4.x, v4.y), fmaxf(v4.z, v4.w)));
-  }
-  return m;
+  // One warp value per lane, then a warp max (redux) in every warp.
+  const unsigned mine = lane < NT / 32 ? __float_as_uint(r[lane]) : 0u;
+  return __uint_as_float(__reduce_max_sync(kFull, mine));
 }
 
 // Block-wide FP64 sum; every thread gets the same value (fixed order).
@@ -738,17 +732,19 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   float *sm_nxt = sp.sm + (par ? 0 : sp.n_sm) * g.PS;
   const float *gl_cur = sp.gl + (par ? GMAX : 0) * g.PS;
   float *gl_nxt = sp.gl + (par ? 0 : GMAX) * g.PS;
-  // lg2 of every regulator gene's current value.  The dense (fast) path
-  // reads an entry only under its slot bit, so entries of genes no link
-  // reads are left unset there; the exact path's slot switch needs them 0.
+  // lg2 of the genes' current values.  The fast path takes it for every
+  // gene of the model (a uniform bound, no per-slot test; its dense slot
+  // masks read only the regulators) and zeroes the slots past the model's
+  // genes; the exact path takes it for the regulators only (lg_mask) and
+  // keeps the other slots 0 for its slot switch.
   float4 lg[NI][GS];
 #pragma unroll
   for (int k = 0; k < GS; ++k) {
-    {
+    if (EXACT || k >= G) {
 #pragma unroll
       for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
     }
-    if (k < G && ((lg_mask >> k) & 1u)) {
+    if (k < G && (!EXACT || ((lg_mask >> k) & 1u))) {
       const float *pl = (k < sp.n_sm ? sm_cur : gl_cur) + k * g.PS;
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
@@ -825,11 +821,11 @@ __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseS
   float4 lg[NI][GS];
 #pragma unroll
   for (int k = 0; k < GS; ++k) {
-    {
+    if (EXACT || k >= G) {
 #pragma unroll
       for (int i = 0; i < NI; ++i) lg[i][k] = f4(0.0f);
     }
-    if (k < G && ((lg_mask >> k) & 1u)) {
+    if (k < G && (!EXACT || ((lg_mask >> k) & 1u))) {
       const float *pl = stage + k * gb.PS;
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
