@@ -709,8 +709,9 @@ def secondary_large(args, grn, torch, local, peaks, peak_kind, n_sm):
     torch.cuda.synchronize()
     pk.status(stream.cuda_stream)
     ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
-    _, _, stats = ev.evaluate_batch(batch.subset(range(8)))
-    plan = ev.autotune_report().splitlines()[-1] if ev.autotune_report() else ""
+    # The plan the autotuner kept for this batch (marked '*' in its report).
+    kept = [l for l in ev.autotune_report().splitlines() if l.lstrip().startswith("*")]
+    plan = kept[-1].lstrip("* ").strip() if kept else None
     pk.free()
     ev.close()
     cells = params["dim_x"] * params["dim_y"]
