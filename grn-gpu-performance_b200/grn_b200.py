@@ -244,7 +244,20 @@ class ModelBatch:
                 self.links[self.link_offsets[i]:self.link_offsets[i + 1]])
 
     def subset(self, idx):
-        return ModelBatch.from_models([self.model(int(i)) for i in idx])
+        """The models at `idx`, in that order (vectorised gather)."""
+        idx = np.asarray(idx, np.int64).reshape(-1)
+
+        def gather(offsets, rows):
+            start, end = offsets[idx].astype(np.int64), offsets[idx + 1].astype(np.int64)
+            lens = end - start
+            out_off = np.zeros(len(idx) + 1, np.int64)
+            np.cumsum(lens, out=out_off[1:])
+            # row r of the result comes from start[m] + (r - out_off[m]) of model m
+            pos = np.arange(out_off[-1]) - np.repeat(out_off[:-1], lens) + np.repeat(start, lens)
+            return out_off, rows[pos]
+        po, prods = gather(self.product_offsets, self.products)
+        lo, links = gather(self.link_offsets, self.links)
+        return ModelBatch(po, prods, lo, links)
 
     def as_c(self):
         c = ModelBatchC()
