@@ -173,6 +173,25 @@ def test_large_256x256_long_run_fp32_vs_fp64():
     assert_raw_close(raw, oraw, what="256x256 1000 steps")
 
 
+def test_large_config_fp32_vs_fp64_full_steps():
+    """The large-grid stress configuration at its full length: 32 seeded
+    models (256 x 256, 8 products, 24 links, dt 0.05, 5000 Euler steps), the
+    FP32 CUDA path against the FP64 oracle on all host cores.  Every model's
+    raw fitness stays within the suite's tolerance (rel 1e-4); the
+    per-model error distribution is printed."""
+    import os
+    params, batch, init, tgt = synth.workload("large_256x256", seed=11, n_models=32)
+    assert params["num_sim_steps"] == 5000 and params["dt"] == 0.05
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        _, raw, _ = ev.evaluate_batch(batch)
+    _, oraw, _ = oracle.evaluate_batch(params, init, tgt, batch, n_threads=os.cpu_count() or 1)
+    rel = np.abs(raw - oraw) / np.maximum(np.abs(oraw), 1e-300)
+    print("FP32 vs FP64, 32 models x 5000 steps: median %.3g, p90 %.3g, max %.3g"
+          % (np.median(rel), np.percentile(rel, 90), rel.max()))
+    assert_raw_close(raw, oraw, what="256x256 5000 steps")
+
+
 def test_schedules_agree_bitwise():
     """Fixed-item, walking-item and all-global-memory schedules run the same
     arithmetic: identical simulated states; the FP64 fitness sums may differ
