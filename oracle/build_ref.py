@@ -112,7 +112,12 @@ def build(force=False, verbose=False):
         cmd = _command(src_root, flags, out)
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        # g++ notes that -I- is obsolete once per source; show its output only
+        # when the build fails.
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("building %s failed" % out)
     return LIB
 
 
