@@ -190,6 +190,10 @@ def run_reference(args, rank, world):
     host cores, rank 0 only."""
     if rank != 0:
         return
+    if args.workload not in synth.WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no %s workload "
+                          "(its surrogate-free CPU evaluator only)" % args.workload}), flush=True)
+        return
     threads = os.cpu_count() or 1
     wl = synth.WORKLOADS[args.workload]
     vals = []
@@ -322,6 +326,69 @@ def run_surrogate_ablation(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_surrogate_mlp(args, rank, world):
+    """The surrogate MLP alone (128 -> 256 -> 256 -> 256 -> 1, ReLU; GEMMs on
+    the tcgen05 tensor cores, BF16 operands, FP32 accumulate), at the C4
+    workload's sizes: screening 8192 offspring per call (forward) and Adam
+    training steps at batch 8192 drawn from a 200k-pair set.
+    FLOPs per row: forward 2 (128*256 + 2*256*256 + 256); a training step
+    3x forward.  A step of this bench is one screening call plus 16 training
+    batches.  Roofline: tensor, against the measured BF16 GEMM peak (burst:
+    each call is timed alone).  Whole calls are timed (host encodings in,
+    predictions out, launches included), so at these sizes the figure shows
+    how far the MLP is from tensor-bound; the ncu summary in profiles/ gives
+    the GEMM kernel itself."""
+    if rank != 0:
+        return
+    import torch
+    import grn_b200 as grn
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(args.seed)
+    n_pairs, screen, batch, n_batches = 200000, 8192, 8192, 16
+    X = (rng.standard_normal((n_pairs, grn.N_FEATURES)) * 0.5).astype(np.float32)
+    y = (0.1 * X[:, :16].sum(1) + 0.05 * rng.standard_normal(n_pairs)).astype(np.float32)
+    Xs = X[:screen].copy()
+    sur = grn.Surrogate(seed=args.seed, capacity=n_pairs)
+    sur.add_data(X, y)
+    fwd = 2 * (128 * 256 + 2 * 256 * 256 + 256)
+    for _ in range(args.warmup):
+        sur.predict(Xs)
+        sur.train_batches(n_batches, batch_size=batch)
+    torch.cuda.synchronize()
+    tp, tt = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sur.predict(Xs)
+        tp.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        sur.train_batches(n_batches, batch_size=batch)
+        tt.append(time.perf_counter() - t0)
+    sur.close()
+    peaks, peak_kind = read_peaks()
+    peak = peaks.get("bf16_tflops", 1590.0)
+    p_s, t_s = statistics.mean(tp), statistics.mean(tt) / n_batches
+    pred_tf = fwd * screen / p_s / 1e12
+    train_tf = 3 * fwd * batch / t_s / 1e12
+    line = {
+        "metric": "surrogate MLP TFLOP/s", "value": train_tf, "unit": "TFLOP/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * (p_s + t_s * n_batches), "higher_is_better": True,
+        "scaling": "none", "vs_baseline": None, "dtype": "bf16 operands, fp32 accumulate",
+        "data": "synthetic",
+        "config": {"workload": "surrogate_mlp", "layers": "128-256-256-256-1 ReLU",
+                   "screen_rows": screen, "train_batch": batch, "pairs": n_pairs,
+                   "step": "one screening call + %d training batches" % n_batches},
+        "screen_ms": 1000 * p_s, "screen_tflops": pred_tf,
+        "train_step_ms": 1000 * t_s, "train_tflops": train_tf,
+        "roofline": {"bound": "tensor", "achieved": train_tf, "peak": peak, "unit": "TFLOP/s",
+                     "frac": train_tf / peak, "traffic": None,
+                     "algorithmic": "3 x 2 x B x (128*256 + 2*256*256 + 256) per training step",
+                     "peak_source": "%s bf16_tflops (burst)" % peak_kind},
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_evolution(args, rank, world):
     """Island evolution workload (islands_100x100: 16 demes x 512 models,
     100x100 grid, <= 8 products and <= 24 links in use, 1500 Euler steps):
@@ -404,7 +471,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="uneven_64x64", choices=sorted(synth.WORKLOADS))
+    ap.add_argument("--workload", default="uneven_64x64",
+                    choices=sorted(synth.WORKLOADS) + ["surrogate_mlp"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--models", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -447,6 +515,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "surrogate_mlp":
+        run_surrogate_mlp(args, rank, world)
         return
     if args.workload == "islands_100x100" and args.surrogate:
         run_surrogate_ablation(args, rank, world)
