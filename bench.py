@@ -328,9 +328,10 @@ def run_surrogate_ablation(args, rank, world):
 
 def run_surrogate_mlp(args, rank, world):
     """The surrogate MLP alone (128 -> 256 -> 256 -> 256 -> 1, ReLU; GEMMs on
-    the tcgen05 tensor cores, BF16 operands, FP32 accumulate), at the C4
-    workload's sizes: screening 8192 offspring per call (forward) and Adam
-    training steps at batch 8192 drawn from a 200k-pair set.
+    the tcgen05 tensor cores fed by a 4-stage TMA ring, BF16 operands, FP32
+    accumulate), at the C4 workload's sizes: screening 8192 offspring per
+    call (forward) and Adam training steps at batch 8192 drawn from a
+    200k-pair set.
     FLOPs per row: forward 2 (128*256 + 2*256*256 + 256); a training step
     3x forward.  A step of this bench is one screening call plus 16 training
     batches.  Roofline: tensor, against the measured BF16 GEMM peak (burst:
@@ -384,7 +385,11 @@ def run_surrogate_mlp(args, rank, world):
                      "frac": train_tf / peak, "traffic": None,
                      "algorithmic": "3 x 2 x B x (128*256 + 2*256*256 + 256) per training step",
                      "peak_source": "%s bf16_tflops (burst)" % peak_kind},
-        "gpu_launches": None,
+        # per step: a screening call (row conversion, 3 GEMMs, output layer)
+        # and per training batch 17 (gather, 3 + 2 GEMMs, 3 weight-gradient
+        # GEMMs with their split-K sums, output layer, loss, last-layer
+        # backward, bias row sums, Adam)
+        "gpu_launches": args.steps * (5 + 17 * n_batches),
     }
     print(json.dumps(line), flush=True)
 

@@ -1,10 +1,14 @@
 // grn_mlp.cu -- kernels of the surrogate fitness model: a 128-256-256-256-1
 // ReLU MLP over a padded encoding of a GRN model, predicting log(error).
 //
-// GEMMs use the tensor cores with BF16 operands and FP32 accumulation
-// (mma.sync m16n8k16); everything else (bias, ReLU masks, loss, reductions,
-// Adam) is plain FP32 SIMT.  No reference counterpart: the reference
-// simulates every offspring.
+// This file holds the warp-level mma.sync GEMM (BF16 operands, FP32
+// accumulation; the legacy tensor-core path, kept to cross-check the
+// tcgen05 GEMM of grn_umma.cu) and the small kernels around the GEMMs:
+// output layer, loss, ReLU-backward of the last layer, bias-gradient row
+// sums, Adam, and the row gathers and transposes that give the tcgen05 GEMM
+// K-major operands.  Every reduction adds in a fixed order, so training is
+// deterministic.  No reference counterpart: the reference simulates every
+// offspring.
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -39,6 +43,8 @@ struct GemmArgs {
   int64_t ldc;
   const float *bias;          // [N] (kEpiBiasRelu)
   const __nv_bfloat16 *mask;  // [M][ldc] (kEpiMask): keep where mask > 0
+  __nv_bfloat16 *Ct;          // optional transposed BF16 output, Ct[n*ldt + m]
+  int64_t ldt;
 };
 
 __device__ __forceinline__ void ldmatrix_x4(uint32_t (&r)[4], const void *p) {
@@ -120,14 +126,19 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
         const int64_t o = (int64_t)m * g.ldc + n;
         if (g.epi == kEpiF32) {
           g.Cf[o] = v;
-        } else if (g.epi == kEpiBiasRelu) {
-          v += g.bias[n];
-          g.Cb[o] = __float2bfloat16(v > 0.0f ? v : 0.0f);
-        } else {  // kEpiMask
-          g.Cb[o] = __float2bfloat16(__bfloat162float(g.mask[o]) > 0.0f ? v : 0.0f);
+        } else {
+          if (g.epi == kEpiBiasRelu) {
+            v += g.bias[n];
+            v = v > 0.0f ? v : 0.0f;
+          } else {  // kEpiMask
+            v = __bfloat162float(g.mask[o]) > 0.0f ? v : 0.0f;
+          }
+          g.Cb[o] = __float2bfloat16(v);
+          if (g.Ct) g.Ct[(int64_t)n * g.ldt + m] = __float2bfloat16(v);
         }
       }
 }
+
 
 // ---- small kernels -----------------------------------------------------
 
@@ -143,59 +154,188 @@ __global__ void output_forward_kernel(int B, int K, const __nv_bfloat16 *h, cons
   if (lane == 0) y[warp] = s + b0[0];
 }
 
-// Loss 1/B sum (y - t)^2 and dy = 2 (y - t) / B.
-__global__ void loss_kernel(int B, const float *y, const float *t, float *dy, double *loss) {
-  __shared__ double part[256];
+// Loss 1/B sum (y - t)^2, dy = 2 (y - t) / B and db = sum dy; one block of
+// kLossThreads, tree sums in a fixed order.  The operands do not alias, so
+// a thread's loads are all issued before its first store.
+constexpr int kLossThreads = 1024;
+
+__global__ void __launch_bounds__(kLossThreads)
+    loss_kernel(int B, const float *__restrict__ y, const float *__restrict__ t,
+                float *__restrict__ dy, double *__restrict__ loss, float *__restrict__ db) {
+  __shared__ double part[kLossThreads];
+  __shared__ float dpart[kLossThreads];
   double s = 0.0;
-  for (int i = threadIdx.x; i < B; i += blockDim.x) {
+  float sd = 0.0f;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < B; i += kLossThreads) {
     const float d = y[i] - t[i];
-    dy[i] = 2.0f * d / (float)B;
+    const float g = 2.0f * d / (float)B;
+    dy[i] = g;
+    sd += g;
     s += (double)d * d;
   }
   part[threadIdx.x] = s;
+  dpart[threadIdx.x] = sd;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      part[threadIdx.x] += part[threadIdx.x + o];
+      dpart[threadIdx.x] += dpart[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double l = part[0] / B;
+    loss[0] = l;
+    loss[1] += l;
+    db[0] = dpart[0];
+  }
+}
+
+// 32 x 32 tiles through shared memory, blocks of 32 x 8 threads: each
+// thread moves four elements of a tile row-wise, then four column-wise, so
+// that the row-major and the transposed stores are both coalesced.
+constexpr int kTile = 32;
+
+// Gradient of the last hidden layer's pre-activation: dz[b][k] =
+// h[b][k] > 0 ? dy[b] w[k] : 0 (BF16), and dzT[k][b].
+__global__ void output_backward_kernel(int B, int K, const __nv_bfloat16 *h, const float *w,
+                                       const float *dy, __nv_bfloat16 *dz, __nv_bfloat16 *dzT,
+                                       int64_t ldt) {
+  __shared__ __nv_bfloat16 tile[kTile][kTile + 2];
+  const int b0 = blockIdx.x * kTile, k0 = blockIdx.y * kTile;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int k = k0 + tx;
+  const float wk = k < K ? w[k] : 0.0f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = ty + 8 * i, b = b0 + r;
+    __nv_bfloat16 v = __float2bfloat16(0.0f);
+    if (b < B && k < K) {
+      const float hv = __bfloat162float(h[(int64_t)b * K + k]);
+      v = __float2bfloat16(hv > 0.0f ? dy[b] * wk : 0.0f);
+      dz[(int64_t)b * K + k] = v;
+    }
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int c = ty + 8 * i, b = b0 + tx;
+    if (k0 + c < K && b < B) dzT[(int64_t)(k0 + c) * ldt + b] = tile[tx][c];
+  }
+}
+
+// Rows to BF16: row r is row idx[r] of the BF16 matrix src_b (a gather), or
+// row r of the FP32 matrix src_f; tdst[r] = tsrc[idx[r]] when gathering.
+// dstT (optional) receives the transpose.
+__global__ void rows_to_bf16_kernel(int rows, int width, const int32_t *idx,
+                                    const __nv_bfloat16 *src_b, const float *src_f,
+                                    const float *tsrc, __nv_bfloat16 *dst, float *tdst,
+                                    __nv_bfloat16 *dstT, int64_t ldt) {
+  __shared__ __nv_bfloat16 tile[kTile][kTile + 2];
+  const int r0 = blockIdx.x * kTile, c0 = blockIdx.y * kTile;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int c = c0 + tx;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = ty + 8 * i, row = r0 + r;
+    __nv_bfloat16 v = __float2bfloat16(0.0f);
+    if (row < rows) {
+      const int64_t s = idx ? (int64_t)idx[row] : (int64_t)row;
+      if (c < width) {
+        v = idx ? src_b[s * width + c] : __float2bfloat16(src_f[s * width + c]);
+        dst[(int64_t)row * width + c] = v;
+      }
+      if (idx && tdst && blockIdx.y == 0 && tx == 0) tdst[row] = tsrc[s];
+    }
+    tile[r][tx] = v;
+  }
+  if (!dstT) return;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int cc = ty + 8 * i, row = r0 + tx;
+    if (c0 + cc < width && row < rows) dstT[(int64_t)(c0 + cc) * ldt + row] = tile[tx][cc];
+  }
+}
+
+// dst[c][r] = src[r][c].
+__global__ void transpose_kernel(int rows, int cols, const __nv_bfloat16 *src, int64_t lds,
+                                 __nv_bfloat16 *dst, int64_t ldd) {
+  __shared__ __nv_bfloat16 tile[kTile][kTile + 2];
+  const int r0 = blockIdx.x * kTile, c0 = blockIdx.y * kTile;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = ty + 8 * i;
+    tile[r][tx] = (r0 + r < rows && c0 + tx < cols) ? src[(int64_t)(r0 + r) * lds + c0 + tx]
+                                                    : __float2bfloat16(0.0f);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int cc = ty + 8 * i;
+    if (c0 + cc < cols && r0 + tx < rows) dst[(int64_t)(c0 + cc) * ldd + r0 + tx] = tile[tx][cc];
+  }
+}
+
+struct RowSumJobs {
+  MlpRowSum j[4];
+};
+
+// out[r] = sum_c X[r][c] (x w[c]): one block of 256 threads per row and
+// job; each thread adds a fixed strided subset, then a fixed-order tree.
+__global__ void __launch_bounds__(256) row_sums_kernel(const RowSumJobs jobs, int cols,
+                                                       int64_t ldx) {
+  __shared__ float part[256];
+  // Selected without a dynamic index into the parameter block (which would
+  // copy it to local memory).
+  const unsigned y = blockIdx.y;
+  const MlpRowSum jb = y == 0 ? jobs.j[0] : y == 1 ? jobs.j[1] : y == 2 ? jobs.j[2] : jobs.j[3];
+  const __nv_bfloat16 *x = jb.X + (int64_t)blockIdx.x * ldx;
+  float s = 0.0f;
+  const bool vec = (cols & 7) == 0 && (ldx & 7) == 0 && ((uintptr_t)jb.X & 15) == 0 &&
+                   (!jb.w || ((uintptr_t)jb.w & 15) == 0);
+  if (vec) {
+    for (int c = threadIdx.x * 8; c < cols; c += 256 * 8) {
+      const uint4 u = *reinterpret_cast<const uint4 *>(x + c);
+      const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&u);
+      float e[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float2 f = __bfloat1622float2(p[q]);
+        e[2 * q] = f.x;
+        e[2 * q + 1] = f.y;
+      }
+      if (jb.w) {
+        const float4 w0 = *reinterpret_cast<const float4 *>(jb.w + c);
+        const float4 w1 = *reinterpret_cast<const float4 *>(jb.w + c + 4);
+        e[0] *= w0.x, e[1] *= w0.y, e[2] *= w0.z, e[3] *= w0.w;
+        e[4] *= w1.x, e[5] *= w1.y, e[6] *= w1.z, e[7] *= w1.w;
+      }
+      s += ((e[0] + e[1]) + (e[2] + e[3])) + ((e[4] + e[5]) + (e[6] + e[7]));
+    }
+  } else {
+    for (int c = threadIdx.x; c < cols; c += 256) {
+      const float v = __bfloat162float(x[c]);
+      s += jb.w ? v * jb.w[c] : v;
+    }
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
     if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *loss = part[0] / B;
+  if (threadIdx.x == 0) jb.out[blockIdx.x] = part[0];
 }
 
-// Gradients of the output layer: dw[k] = sum_b dy[b] h[b][k], db = sum dy,
-// and dz[b][k] = dy[b] w[k] where h[b][k] > 0 (BF16, next backward GEMM).
-__global__ void output_backward_kernel(int B, int K, const __nv_bfloat16 *h, const float *w,
-                                       const float *dy, float *dw, float *db,
-                                       __nv_bfloat16 *dz) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < K) {
-    float s = 0.0f;
-    for (int b = 0; b < B; ++b) {
-      const float hv = __bfloat162float(h[(int64_t)b * K + k]);
-      s += dy[b] * hv;
-      dz[(int64_t)b * K + k] = __float2bfloat16(hv > 0.0f ? dy[b] * w[k] : 0.0f);
-    }
-    dw[k] = s;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    float s = 0.0f;
-    for (int b = 0; b < B; ++b) s += dy[b];
-    db[0] = s;
-  }
-}
-
-// db[n] = sum_b dz[b][n] (bias gradients of the hidden layers).
-__global__ void column_sum_kernel(int B, int N, const __nv_bfloat16 *dz, float *db) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  float s = 0.0f;
-  for (int b = 0; b < B; ++b) s += __bfloat162float(dz[(int64_t)b * N + n]);
-  db[n] = s;
-}
-
-// Adam on FP32 master weights; refreshes the BF16 copy.
+// Adam on FP32 master weights; refreshes the BF16 copy and the transposed
+// BF16 copies of the square matrices listed in tr.
 __global__ void adam_kernel(int n, float *w, const float *g, float *m, float *v, float lr,
                             float b1, float b2, float eps, float c1, float c2,
-                            __nv_bfloat16 *wb) {
+                            __nv_bfloat16 *wb, const MlpTransposed tr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float gi = g[i];
@@ -205,7 +345,18 @@ __global__ void adam_kernel(int n, float *w, const float *g, float *m, float *v,
   v[i] = vi;
   const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
   w[i] = wi;
-  if (wb) wb[i] = __float2bfloat16(wi);
+  if (!wb) return;
+  const __nv_bfloat16 wv = __float2bfloat16(wi);
+  wb[i] = wv;
+  const int64_t nn = (int64_t)tr.n * tr.n;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int64_t o = i - tr.offset[j];
+    if (tr.dst[j] && o >= 0 && o < nn) {
+      const int r = (int)(o / tr.n), c = (int)(o - (int64_t)r * tr.n);
+      tr.dst[j][(int64_t)c * tr.n + r] = wv;
+    }
+  }
 }
 
 __global__ void to_bf16_kernel(int n, const float *x, __nv_bfloat16 *y) {
@@ -213,58 +364,57 @@ __global__ void to_bf16_kernel(int n, const float *x, __nv_bfloat16 *y) {
   if (i < n) y[i] = __float2bfloat16(x[i]);
 }
 
-// out[r] = src[idx[r]] rows of `width` (training minibatch gather).
-__global__ void gather_rows_kernel(int rows, int width, const int32_t *idx,
-                                   const __nv_bfloat16 *src, const float *tsrc,
-                                   __nv_bfloat16 *dst, float *tdst) {
-  const int r = blockIdx.x;
-  if (r >= rows) return;
-  const int64_t s = idx[r];
-  for (int c = threadIdx.x; c < width; c += blockDim.x)
-    dst[(int64_t)r * width + c] = src[s * width + c];
-  if (threadIdx.x == 0) tdst[r] = tsrc[s];
+dim3 tile_grid(int rows, int cols) {
+  return dim3((rows + kTile - 1) / kTile, (cols + kTile - 1) / kTile);
 }
 
 }  // namespace
 
-cudaError_t mlp_gemm(int M, int N, int K, const __nv_bfloat16 *A, int64_t a_rs, int64_t a_cs,
-                     const __nv_bfloat16 *B, int64_t b_rs, int64_t b_cs, int epi, float *Cf,
-                     __nv_bfloat16 *Cb, int64_t ldc, const float *bias,
-                     const __nv_bfloat16 *mask, cudaStream_t st) {
-  GemmArgs g{M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, epi, Cf, Cb, ldc, bias, mask};
-  dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM);
+cudaError_t mlp_gemm(const MlpGemm &p, cudaStream_t st) {
+  if (p.M < 1 || p.N < 1 || p.K < 1) return cudaErrorInvalidValue;
+  GemmArgs g{p.M, p.N, p.K, p.A, p.lda, 1, p.B, p.ldb, 1, p.epi, p.Cf, p.Cb, p.ldc,
+             p.bias, p.mask, p.Ct, p.ldt};
+  dim3 grid((p.N + kTN - 1) / kTN, (p.M + kTM - 1) / kTM);
   gemm_bf16_kernel<<<grid, 128, 0, st>>>(g);
   return cudaGetLastError();
 }
 
 cudaError_t mlp_output_forward(int B, int K, const __nv_bfloat16 *h, const float *w,
                                const float *b0, float *y, cudaStream_t st) {
+  if (B < 1) return cudaSuccess;
   output_forward_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(B, K, h, w, b0, y);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_loss(int B, const float *y, const float *t, float *dy, double *loss,
+cudaError_t mlp_loss(int B, const float *y, const float *t, float *dy, double *loss, float *db,
                      cudaStream_t st) {
-  loss_kernel<<<1, 256, 0, st>>>(B, y, t, dy, loss);
+  loss_kernel<<<1, kLossThreads, 0, st>>>(B, y, t, dy, loss, db);
   return cudaGetLastError();
 }
 
 cudaError_t mlp_output_backward(int B, int K, const __nv_bfloat16 *h, const float *w,
-                                const float *dy, float *dw, float *db, __nv_bfloat16 *dz,
-                                cudaStream_t st) {
-  output_backward_kernel<<<(K + 127) / 128, 128, 0, st>>>(B, K, h, w, dy, dw, db, dz);
+                                const float *dy, __nv_bfloat16 *dz, __nv_bfloat16 *dzT,
+                                int64_t ldt, cudaStream_t st) {
+  if (B < 1 || K < 1) return cudaSuccess;
+  output_backward_kernel<<<tile_grid(B, K), dim3(kTile, 8), 0, st>>>(B, K, h, w, dy, dz, dzT,
+                                                                     ldt);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_column_sum(int B, int N, const __nv_bfloat16 *dz, float *db, cudaStream_t st) {
-  column_sum_kernel<<<(N + 127) / 128, 128, 0, st>>>(B, N, dz, db);
+cudaError_t mlp_row_sums(int n_jobs, const MlpRowSum *jobs, int rows, int cols, int64_t ldx,
+                         cudaStream_t st) {
+  if (n_jobs < 1 || n_jobs > 4 || rows < 1) return cudaErrorInvalidValue;
+  RowSumJobs j{};
+  for (int i = 0; i < n_jobs; ++i) j.j[i] = jobs[i];
+  row_sums_kernel<<<dim3(rows, n_jobs), 256, 0, st>>>(j, cols, ldx);
   return cudaGetLastError();
 }
 
 cudaError_t mlp_adam(int n, float *w, const float *g, float *m, float *v, float lr, float b1,
-                     float b2, float eps, int t, __nv_bfloat16 *wb, cudaStream_t st) {
+                     float b2, float eps, int t, __nv_bfloat16 *wb, const MlpTransposed &tr,
+                     cudaStream_t st) {
   const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
-  adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, g, m, v, lr, b1, b2, eps, c1, c2, wb);
+  adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, g, m, v, lr, b1, b2, eps, c1, c2, wb, tr);
   return cudaGetLastError();
 }
 
@@ -273,11 +423,28 @@ cudaError_t mlp_to_bf16(int n, const float *x, __nv_bfloat16 *y, cudaStream_t st
   return cudaGetLastError();
 }
 
+cudaError_t mlp_transpose(int rows, int cols, const __nv_bfloat16 *src, int64_t lds,
+                          __nv_bfloat16 *dst, int64_t ldd, cudaStream_t st) {
+  if (rows < 1 || cols < 1) return cudaSuccess;
+  transpose_kernel<<<tile_grid(rows, cols), dim3(kTile, 8), 0, st>>>(rows, cols, src, lds, dst,
+                                                                     ldd);
+  return cudaGetLastError();
+}
+
 cudaError_t mlp_gather_rows(int rows, int width, const int32_t *idx, const __nv_bfloat16 *src,
                             const float *tsrc, __nv_bfloat16 *dst, float *tdst,
-                            cudaStream_t st) {
-  if (rows == 0) return cudaSuccess;
-  gather_rows_kernel<<<rows, 128, 0, st>>>(rows, width, idx, src, tsrc, dst, tdst);
+                            __nv_bfloat16 *dstT, int64_t ldt, cudaStream_t st) {
+  if (rows < 1) return cudaSuccess;
+  rows_to_bf16_kernel<<<tile_grid(rows, width), dim3(kTile, 8), 0, st>>>(
+      rows, width, idx, src, nullptr, tsrc, dst, tdst, dstT, ldt);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_convert_rows(int rows, int width, const float *src, __nv_bfloat16 *dst,
+                             __nv_bfloat16 *dstT, int64_t ldt, cudaStream_t st) {
+  if (rows < 1) return cudaSuccess;
+  rows_to_bf16_kernel<<<tile_grid(rows, width), dim3(kTile, 8), 0, st>>>(
+      rows, width, nullptr, nullptr, src, nullptr, dst, nullptr, dstT, ldt);
   return cudaGetLastError();
 }
 

@@ -44,12 +44,21 @@ struct grn_surrogate {
   cudaStream_t st = nullptr;
   float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   __nv_bfloat16 *wb = nullptr;
+  __nv_bfloat16 *w2t = nullptr, *w3t = nullptr;  // transposed BF16 W2, W3
   int bmax = 0;
+  // Minibatch activations and gradients, row-major [bmax][width], and their
+  // transposes [width][bmax] (the K-major operands of the weight gradients).
   __nv_bfloat16 *x = nullptr, *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;
   __nv_bfloat16 *dz1 = nullptr, *dz2 = nullptr, *dz3 = nullptr;
+  __nv_bfloat16 *xT = nullptr, *h1T = nullptr, *h2T = nullptr, *h3T = nullptr;
+  __nv_bfloat16 *dz1T = nullptr, *dz2T = nullptr, *dz3T = nullptr;
+  float *xf = nullptr;  // FP32 staging of uploaded rows [bmax][kF]
   float *y = nullptr, *t = nullptr, *dy = nullptr;
-  double *loss = nullptr;
+  double *loss = nullptr;  // [0] last minibatch, [1] sum over a training call
+  float *work = nullptr;   // split-K partial tiles of the weight gradients
+  size_t work_elems = 0;
   int32_t *idx = nullptr;
+  int idx_cap = 0;
   int cap = 0, count = 0, head = 0;  // dataset ring buffer
   __nv_bfloat16 *dx = nullptr;
   float *dt = nullptr;
@@ -61,16 +70,23 @@ struct grn_surrogate {
 
 namespace {
 
+grn::MlpGemm gemm_args(int M, int N, int K, const __nv_bfloat16 *A, int64_t lda,
+                       const __nv_bfloat16 *B, int64_t ldb) {
+  grn::MlpGemm p{};
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.A = A;
+  p.lda = lda;
+  p.B = B;
+  p.ldb = ldb;
+  return p;
+}
+
 // One GEMM of the MLP on the selected tensor-core path.
-cudaError_t gemm(grn_surrogate *s, int M, int N, int K, const __nv_bfloat16 *A, int64_t a_rs,
-                 int64_t a_cs, const __nv_bfloat16 *B, int64_t b_rs, int64_t b_cs, int epi,
-                 float *Cf, __nv_bfloat16 *Cb, int64_t ldc, const float *bias,
-                 const __nv_bfloat16 *mask) {
-  if (s->tcgen05)
-    return grn::mlp_gemm_tc(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, epi, Cf, Cb, ldc, bias, mask,
-                            s->d_err, s->st);
-  return grn::mlp_gemm(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, epi, Cf, Cb, ldc, bias, mask,
-                       s->st);
+cudaError_t gemm(grn_surrogate *s, const grn::MlpGemm &p) {
+  if (s->tcgen05) return grn::mlp_gemm_tc(p, s->work, s->work_elems, s->d_err, s->st);
+  return grn::mlp_gemm(p, s->st);
 }
 
 // Reads and clears the tcgen05 time-out flag (after the stream is synced).
@@ -82,69 +98,129 @@ grn_status check_err(grn_surrogate *s) {
   return GRN_ERR_KERNEL;
 }
 
-grn_status forward(grn_surrogate *s, int B) {
+// Hidden layers and output of the rows in s->x; `train` also stores the
+// transposed activations that the weight gradients read.
+grn_status forward(grn_surrogate *s, int B, bool train) {
   using namespace grn;
-  cudaStream_t st = s->st;
-  GRN_CK(gemm(s, B, kH, kF, s->x, kF, 1, s->wb + kW1, kF, 1, kEpiBiasRelu, nullptr, s->h1, kH,
-                  s->w + kB1, nullptr));
-  GRN_CK(gemm(s, B, kH, kH, s->h1, kH, 1, s->wb + kW2, kH, 1, kEpiBiasRelu, nullptr, s->h2, kH,
-                  s->w + kB2, nullptr));
-  GRN_CK(gemm(s, B, kH, kH, s->h2, kH, 1, s->wb + kW3, kH, 1, kEpiBiasRelu, nullptr, s->h3, kH,
-                  s->w + kB3, nullptr));
-  GRN_CK(mlp_output_forward(B, kH, s->h3, s->w + kW4, s->w + kB4, s->y, st));
+  const int64_t T = s->bmax;
+  const __nv_bfloat16 *in[3] = {s->x, s->h1, s->h2};
+  __nv_bfloat16 *out[3] = {s->h1, s->h2, s->h3}, *outT[3] = {s->h1T, s->h2T, s->h3T};
+  const int64_t wo[3] = {kW1, kW2, kW3}, bo[3] = {kB1, kB2, kB3};
+  for (int l = 0; l < 3; ++l) {
+    const int K = l == 0 ? kF : kH;
+    MlpGemm p = gemm_args(B, kH, K, in[l], K, s->wb + wo[l], K);
+    p.epi = kEpiBiasRelu;
+    p.Cb = out[l];
+    p.ldc = kH;
+    p.bias = s->w + bo[l];
+    if (train) {
+      p.Ct = outT[l];
+      p.ldt = T;
+    }
+    GRN_CK(gemm(s, p));
+  }
+  GRN_CK(mlp_output_forward(B, kH, s->h3, s->w + kW4, s->w + kB4, s->y, s->st));
   return GRN_OK;
 }
 
-// Loss and gradients of a minibatch already in s->x / s->t (after forward).
+// Loss and gradients of a minibatch already in s->x / s->xT / s->t (after
+// forward with train set).
 grn_status backward(grn_surrogate *s, int B) {
   using namespace grn;
   cudaStream_t st = s->st;
-  GRN_CK(mlp_loss(B, s->y, s->t, s->dy, s->loss, st));
-  GRN_CK(mlp_output_backward(B, kH, s->h3, s->w + kW4, s->dy, s->g + kW4, s->g + kB4, s->dz3,
-                             st));
-  // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * [H2 > 0]
-  GRN_CK(gemm(s, kH, kH, B, s->dz3, 1, kH, s->h2, 1, kH, kEpiF32, s->g + kW3, nullptr, kH,
-                  nullptr, nullptr));
-  GRN_CK(mlp_column_sum(B, kH, s->dz3, s->g + kB3, st));
-  GRN_CK(gemm(s, B, kH, kH, s->dz3, kH, 1, s->wb + kW3, 1, kH, kEpiMask, nullptr, s->dz2, kH,
-                  nullptr, s->h2));
-  // layer 2
-  GRN_CK(gemm(s, kH, kH, B, s->dz2, 1, kH, s->h1, 1, kH, kEpiF32, s->g + kW2, nullptr, kH,
-                  nullptr, nullptr));
-  GRN_CK(mlp_column_sum(B, kH, s->dz2, s->g + kB2, st));
-  GRN_CK(gemm(s, B, kH, kH, s->dz2, kH, 1, s->wb + kW2, 1, kH, kEpiMask, nullptr, s->dz1, kH,
-                  nullptr, s->h1));
-  // layer 1: dW1 = dZ1^T X (no input gradient needed)
-  GRN_CK(gemm(s, kH, kF, B, s->dz1, 1, kH, s->x, 1, kF, kEpiF32, s->g + kW1, nullptr, kF,
-                  nullptr, nullptr));
-  GRN_CK(mlp_column_sum(B, kH, s->dz1, s->g + kB1, st));
+  const int64_t T = s->bmax;
+  GRN_CK(mlp_loss(B, s->y, s->t, s->dy, s->loss, s->g + kB4, st));
+  GRN_CK(mlp_output_backward(B, kH, s->h3, s->w + kW4, s->dy, s->dz3, s->dz3T, T, st));
+  // Per hidden layer l = 3, 2, 1: dW_l = dZ_l^T H_(l-1) (K = the batch, from
+  // the transposed copies), and for l > 1 dZ_(l-1) = (dZ_l W_l) * [H_(l-1) > 0].
+  const __nv_bfloat16 *dzT[3] = {s->dz1T, s->dz2T, s->dz3T};
+  const __nv_bfloat16 *hT[3] = {s->xT, s->h1T, s->h2T};
+  const __nv_bfloat16 *dz[3] = {s->dz1, s->dz2, s->dz3};
+  const __nv_bfloat16 *hprev[3] = {s->x, s->h1, s->h2};
+  const __nv_bfloat16 *wt[3] = {nullptr, s->w2t, s->w3t};
+  __nv_bfloat16 *dzo[3] = {nullptr, s->dz1, s->dz2}, *dzoT[3] = {nullptr, s->dz1T, s->dz2T};
+  const int64_t wo[3] = {kW1, kW2, kW3};
+  for (int l = 2; l >= 0; --l) {
+    const int N = l == 0 ? kF : kH;
+    MlpGemm p = gemm_args(kH, N, B, dzT[l], T, hT[l], T);
+    p.epi = kEpiF32;
+    p.Cf = s->g + wo[l];
+    p.ldc = N;
+    GRN_CK(gemm(s, p));
+    if (l == 0) break;
+    p = gemm_args(B, kH, kH, dz[l], kH, wt[l], kH);
+    p.epi = kEpiMask;
+    p.Cb = dzo[l];
+    p.ldc = kH;
+    p.mask = hprev[l];
+    p.Ct = dzoT[l];
+    p.ldt = T;
+    GRN_CK(gemm(s, p));
+  }
+  // Output weights and hidden biases: sums over the batch of the transposes.
+  const MlpRowSum jobs[4] = {{s->h3T, s->dy, s->g + kW4},
+                             {s->dz3T, nullptr, s->g + kB3},
+                             {s->dz2T, nullptr, s->g + kB2},
+                             {s->dz1T, nullptr, s->g + kB1}};
+  GRN_CK(mlp_row_sums(4, jobs, kH, B, T, st));
   return GRN_OK;
 }
 
-// One Adam step on the training-set rows idx[0..B); adds its loss to *loss_sum.
-grn_status train_minibatch(grn_surrogate *s, const int32_t *idx, int B, float lr,
-                           double *loss_sum) {
-  GRN_CK(cudaMemcpyAsync(s->idx, idx, (size_t)B * 4, cudaMemcpyHostToDevice, s->st));
-  GRN_CK(grn::mlp_gather_rows(B, kF, s->idx, s->dx, s->dt, s->x, s->t, s->st));
-  grn_status st = forward(s, B);
+// Refreshes the transposed BF16 weights the backward GEMMs read (after the
+// parameters are set; Adam refreshes them after each step).
+grn_status transpose_weights(grn_surrogate *s) {
+  GRN_CK(grn::mlp_transpose(kH, kH, s->wb + kW2, kH, s->w2t, kH, s->st));
+  GRN_CK(grn::mlp_transpose(kH, kH, s->wb + kW3, kH, s->w3t, kH, s->st));
+  return GRN_OK;
+}
+
+// One Adam step on the training-set rows d_idx[0..B) (device indices).
+grn_status train_minibatch(grn_surrogate *s, const int32_t *d_idx, int B, float lr) {
+  GRN_CK(grn::mlp_gather_rows(B, kF, d_idx, s->dx, s->dt, s->x, s->t, s->xT, s->bmax, s->st));
+  grn_status st = forward(s, B, true);
   if (st == GRN_OK) st = backward(s, B);
   if (st != GRN_OK) return st;
   s->step += 1;
+  const grn::MlpTransposed tr{{kW2, kW3}, {s->w2t, s->w3t}, kH};
   GRN_CK(grn::mlp_adam((int)kP, s->w, s->g, s->m, s->v, lr, 0.9f, 0.999f, 1e-8f, s->step, s->wb,
-                       s->st));
-  double l = 0;
-  GRN_CK(cudaMemcpyAsync(&l, s->loss, 8, cudaMemcpyDeviceToHost, s->st));
-  GRN_CK(cudaStreamSynchronize(s->st));
-  *loss_sum += l;
+                       tr, s->st));
   return GRN_OK;
 }
 
-grn_status upload_features(grn_surrogate *s, const float *features, int n, __nv_bfloat16 *dst) {
-  std::vector<__nv_bfloat16> hb((size_t)n * kF);
-  for (size_t i = 0; i < hb.size(); ++i) hb[i] = __float2bfloat16(features[i]);
-  GRN_CK(cudaMemcpyAsync(dst, hb.data(), hb.size() * sizeof(__nv_bfloat16),
-                         cudaMemcpyHostToDevice, s->st));
+// Runs minibatch i on the sizes[i] training-set rows that follow in idx.
+// Indices go to the device in chunks of whole minibatches, and the losses
+// add up on the device: one host synchronisation per call.
+grn_status run_minibatches(grn_surrogate *s, const std::vector<int32_t> &idx,
+                           const std::vector<int> &sizes, float lr, double *mean_loss) {
+  GRN_CK(cudaMemsetAsync(s->loss + 1, 0, sizeof(double), s->st));
+  size_t pos = 0, b = 0;
+  while (b < sizes.size()) {
+    size_t e = b, rows = 0;
+    while (e < sizes.size() && rows + sizes[e] <= (size_t)s->idx_cap) rows += sizes[e++];
+    GRN_CK(cudaMemcpyAsync(s->idx, idx.data() + pos, rows * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, s->st));
+    size_t off = 0;
+    for (; b < e; ++b) {
+      const grn_status st = train_minibatch(s, s->idx + off, sizes[b], lr);
+      if (st != GRN_OK) return st;
+      off += sizes[b];
+    }
+    pos += rows;
+  }
+  double l = 0;
+  GRN_CK(cudaMemcpyAsync(&l, s->loss + 1, sizeof l, cudaMemcpyDeviceToHost, s->st));
   GRN_CK(cudaStreamSynchronize(s->st));
+  if (mean_loss) *mean_loss = sizes.empty() ? 0 : l / sizes.size();
+  return GRN_OK;
+}
+
+// n <= bmax FP32 rows of kF features from the host to BF16 rows at dst (and
+// their transpose at dstT, if set), through the FP32 staging buffer.
+grn_status stage_rows(grn_surrogate *s, const float *features, int n, __nv_bfloat16 *dst,
+                      __nv_bfloat16 *dstT) {
+  GRN_CK(cudaMemcpyAsync(s->xf, features, (size_t)n * kF * sizeof(float), cudaMemcpyHostToDevice,
+                         s->st));
+  GRN_CK(grn::mlp_convert_rows(n, kF, s->xf, dst, dstT, s->bmax, s->st));
   return GRN_OK;
 }
 
@@ -223,15 +299,23 @@ grn_status grn_surrogate_create(int device, uint64_t seed, int capacity, grn_sur
   alloc((void **)&s->m, kP * 4);
   alloc((void **)&s->v, kP * 4);
   alloc((void **)&s->wb, kP * 2);
+  alloc((void **)&s->w2t, (size_t)kH * kH * 2);
+  alloc((void **)&s->w3t, (size_t)kH * kH * 2);
   const size_t B = s->bmax;
-  alloc((void **)&s->x, B * kF * 2);
-  for (__nv_bfloat16 **p : {&s->h1, &s->h2, &s->h3, &s->dz1, &s->dz2, &s->dz3})
+  for (__nv_bfloat16 **p : {&s->x, &s->xT}) alloc((void **)p, B * kF * 2);
+  for (__nv_bfloat16 **p : {&s->h1, &s->h2, &s->h3, &s->dz1, &s->dz2, &s->dz3, &s->h1T, &s->h2T,
+                            &s->h3T, &s->dz1T, &s->dz2T, &s->dz3T})
     alloc((void **)p, B * kH * 2);
+  alloc((void **)&s->xf, B * kF * 4);
   alloc((void **)&s->y, B * 4);
   alloc((void **)&s->t, B * 4);
   alloc((void **)&s->dy, B * 4);
-  alloc((void **)&s->loss, 8);
-  alloc((void **)&s->idx, B * 4);
+  alloc((void **)&s->loss, 2 * sizeof(double));
+  // Split-K workspace: 32 partial 256 x 256 FP32 tiles.
+  s->work_elems = (size_t)32 * kH * kH;
+  alloc((void **)&s->work, s->work_elems * 4);
+  s->idx_cap = 16 * s->bmax;
+  alloc((void **)&s->idx, (size_t)s->idx_cap * 4);
   alloc((void **)&s->dx, (size_t)capacity * kF * 2);
   alloc((void **)&s->dt, (size_t)capacity * 4);
   alloc((void **)&s->d_err, sizeof(int));
@@ -264,10 +348,12 @@ grn_status grn_surrogate_destroy(grn_surrogate *s) {
   cudaSetDevice(s->device);
   if (s->st) cudaStreamSynchronize(s->st);
   for (void *p : {(void *)s->w, (void *)s->g, (void *)s->m, (void *)s->v, (void *)s->wb,
-                  (void *)s->x, (void *)s->h1, (void *)s->h2, (void *)s->h3, (void *)s->dz1,
-                  (void *)s->dz2, (void *)s->dz3, (void *)s->y, (void *)s->t, (void *)s->dy,
-                  (void *)s->loss, (void *)s->idx, (void *)s->dx, (void *)s->dt,
-                  (void *)s->d_err})
+                  (void *)s->w2t, (void *)s->w3t, (void *)s->x, (void *)s->h1, (void *)s->h2,
+                  (void *)s->h3, (void *)s->dz1, (void *)s->dz2, (void *)s->dz3, (void *)s->xT,
+                  (void *)s->h1T, (void *)s->h2T, (void *)s->h3T, (void *)s->dz1T,
+                  (void *)s->dz2T, (void *)s->dz3T, (void *)s->xf, (void *)s->y, (void *)s->t,
+                  (void *)s->dy, (void *)s->loss, (void *)s->work, (void *)s->idx, (void *)s->dx,
+                  (void *)s->dt, (void *)s->d_err})
     if (p) cudaFree(p);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
@@ -281,6 +367,8 @@ grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n
   GRN_CK(cudaMemsetAsync(s->m, 0, kP * 4, s->st));
   GRN_CK(cudaMemsetAsync(s->v, 0, kP * 4, s->st));
   GRN_CK(grn::mlp_to_bf16((int)kP, s->w, s->wb, s->st));
+  const grn_status ts = transpose_weights(s);
+  if (ts != GRN_OK) return ts;
   GRN_CK(cudaStreamSynchronize(s->st));
   s->step = 0;
   return GRN_OK;
@@ -299,17 +387,17 @@ grn_status grn_surrogate_add_data(grn_surrogate *s, const float *features, const
   if (!s || n < 0 || (n > 0 && (!features || !log_error))) return GRN_ERR_INVALID_ARGUMENT;
   cudaSetDevice(s->device);
   for (int i = 0; i < n;) {
-    const int chunk = std::min(n - i, s->cap - s->head);
-    grn_status st = upload_features(s, features + (size_t)i * kF, chunk,
-                                    s->dx + (size_t)s->head * kF);
+    const int chunk = std::min({n - i, s->cap - s->head, s->bmax});
+    const grn_status st = stage_rows(s, features + (size_t)i * kF, chunk,
+                                     s->dx + (size_t)s->head * kF, nullptr);
     if (st != GRN_OK) return st;
     GRN_CK(cudaMemcpyAsync(s->dt + s->head, log_error + i, chunk * 4, cudaMemcpyHostToDevice,
                            s->st));
-    GRN_CK(cudaStreamSynchronize(s->st));
     s->head = (s->head + chunk) % s->cap;
     s->count = std::min(s->cap, s->count + chunk);
     i += chunk;
   }
+  GRN_CK(cudaStreamSynchronize(s->st));
   return GRN_OK;
 }
 
@@ -321,20 +409,18 @@ grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, flo
     return GRN_ERR_INVALID_ARGUMENT;
   if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
   cudaSetDevice(s->device);
-  std::vector<int32_t> perm(s->count);
-  double loss_sum = 0;
-  long n_batches = 0;
+  std::vector<int32_t> perm(s->count), idx;
+  std::vector<int> sizes;
+  idx.reserve((size_t)epochs * s->count);
   for (int e = 0; e < epochs; ++e) {
     for (int i = 0; i < s->count; ++i) perm[i] = i;
     std::shuffle(perm.begin(), perm.end(), s->rng);
-    for (int b0 = 0; b0 < s->count; b0 += batch_size) {
-      const int B = std::min(batch_size, s->count - b0);
-      grn_status st = train_minibatch(s, perm.data() + b0, B, lr, &loss_sum);
-      if (st != GRN_OK) return st;
-      ++n_batches;
-    }
+    idx.insert(idx.end(), perm.begin(), perm.end());
+    for (int b0 = 0; b0 < s->count; b0 += batch_size)
+      sizes.push_back(std::min(batch_size, s->count - b0));
   }
-  if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
+  const grn_status st = run_minibatches(s, idx, sizes, lr, mean_loss);
+  if (st != GRN_OK) return st;
   return check_err(s);
 }
 
@@ -345,15 +431,11 @@ grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batc
   if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
   cudaSetDevice(s->device);
   const int B = std::min(batch_size, s->count);
-  std::vector<int32_t> idx(B);
+  std::vector<int32_t> idx((size_t)n_batches * B);
   std::uniform_int_distribution<int32_t> pick(0, s->count - 1);
-  double loss_sum = 0;
-  for (int it = 0; it < n_batches; ++it) {
-    for (int i = 0; i < B; ++i) idx[i] = pick(s->rng);
-    grn_status st = train_minibatch(s, idx.data(), B, lr, &loss_sum);
-    if (st != GRN_OK) return st;
-  }
-  if (mean_loss) *mean_loss = n_batches ? loss_sum / n_batches : 0;
+  for (auto &i : idx) i = pick(s->rng);
+  const grn_status st = run_minibatches(s, idx, std::vector<int>(n_batches, B), lr, mean_loss);
+  if (st != GRN_OK) return st;
   return check_err(s);
 }
 
@@ -362,8 +444,8 @@ grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n,
   cudaSetDevice(s->device);
   for (int i = 0; i < n; i += s->bmax) {
     const int B = std::min(s->bmax, n - i);
-    grn_status st = upload_features(s, features + (size_t)i * kF, B, s->x);
-    if (st == GRN_OK) st = forward(s, B);
+    grn_status st = stage_rows(s, features + (size_t)i * kF, B, s->x, nullptr);
+    if (st == GRN_OK) st = forward(s, B, false);
     if (st != GRN_OK) return st;
     GRN_CK(cudaMemcpyAsync(out + i, s->y, B * 4, cudaMemcpyDeviceToHost, s->st));
     GRN_CK(cudaStreamSynchronize(s->st));
@@ -382,10 +464,10 @@ grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
   if (!s || !features || !log_error || !grads || n < 1 || n > s->bmax)
     return GRN_ERR_INVALID_ARGUMENT;
   cudaSetDevice(s->device);
-  grn_status st = upload_features(s, features, n, s->x);
+  grn_status st = stage_rows(s, features, n, s->x, s->xT);
   if (st != GRN_OK) return st;
   GRN_CK(cudaMemcpyAsync(s->t, log_error, n * 4, cudaMemcpyHostToDevice, s->st));
-  st = forward(s, n);
+  st = forward(s, n, true);
   if (st == GRN_OK) st = backward(s, n);
   if (st != GRN_OK) return st;
   GRN_CK(cudaMemcpyAsync(grads, s->g, kP * 4, cudaMemcpyDeviceToHost, s->st));
