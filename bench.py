@@ -414,6 +414,8 @@ def run_evolution(args, rank, world):
                  n_max_links=24, n_host_threads=0, seed=args.seed + rank)
     ev = grn.Evaluator(params, device=torch.cuda.current_device())
     ev.set_experiments(init, tgt)
+    if args.schedule != "auto":
+        ev.set_schedule({v: k for k, v in grn.SCHEDULE_NAMES.items()}[args.schedule])
     evo = grn.Evolution(evo_p, wl["n_in"] + wl["n_target"], evaluator=ev)
     if args.skip_clones:
         evo.set_skip_clones(True)
@@ -465,6 +467,8 @@ def run_evolution(args, rank, world):
             "final_best_error": final_best,
             "time_to_best_within_1pct_s": t_target,
             "generation_reaching_it": g_target,
+            # the autotuner's candidates and times ('*' = kept), per batch shape
+            "autotune": [l.strip() for l in ev.autotune_report().splitlines() if l.strip()],
         }
         print(json.dumps(line), flush=True)
     evo.close()

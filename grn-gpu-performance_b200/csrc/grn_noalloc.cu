@@ -116,7 +116,8 @@ extern "C" grn_status grn_evaluate_batch_noalloc(
   std::string perr;
   unsigned hw = std::thread::hardware_concurrency();
   grn_status s = pack_batch(batch, params->n_input_morphogens + params->n_target_morphogens,
-                            hw ? (int)hw : 1, &ph, &perr);
+                            (float)params->dt, params->num_sim_steps, hw ? (int)hw : 1, &ph,
+                            &perr);
   if (s != GRN_OK) return put_error(err_buf, err_buf_len, s, perr);
 
   // Scratch layout: [counter, flag] | records | offsets | state slots.

@@ -38,9 +38,9 @@ constexpr uint32_t kFlagNone = 0u;
 // 0 < K^n <= 1e300, every gene finite rates, and no (regulator, regulated)
 // pair repeats: on a bounded non-negative state no link term can be NaN, so
 // the kernel may combine terms with min/max over a dense per-gene table of
-// regulator slots (see the kernel's regulation).  The kernel also requires
-// the step size to keep the state bounded (euler_bounded) before it takes
-// the fast path.
+// regulator slots (see the kernel's regulation).  pack_batch also clears
+// the flag where the run's step size could leave the state unbounded
+// (euler_bounded in host/pack.h), so the kernel tests only the flag.
 constexpr uint32_t kFlagFast = 1u;
 
 struct alignas(16) PackedHeader {

@@ -276,9 +276,10 @@ __device__ __forceinline__ bool chk_copy(const float *dst, const float *src, lon
 // its links (grn_packed.h).  Two combine modes:
 //   fast   min / max (fminf / fmaxf).  Identical to the reference whenever
 //          no link term is NaN, which holds for models with finite K > 0,
-//          finite Hill coefficients and 0 < K^n <= 1e300 (flag kFlagFast) on
-//          bounded non-negative states (euler_bounded and the host's
-//          fast_ok).
+//          finite Hill coefficients and 0 < K^n <= 1e300 on bounded
+//          non-negative states (flag kFlagFast, which the host also clears
+//          for a step size that could leave the state unbounded, and the
+//          context's fast_ok for the initial states).
 //   exact  the reference's comparison order (simopor.cpp:20-22,
 //          simopand.cpp:20-22 with MathAlgo::max/min): a NaN term on
 //          either side yields the new term; a NaN start makes the first
@@ -531,31 +532,6 @@ __device__ __forceinline__ int cell_offset(const Geom &g, int y, int x) {
   return (y + 1) * g.RS + x;
 }
 
-// Whether a fast-flagged model may run the fast path at this step size.
-// The fast path needs a state that stays finite and non-negative.  With
-// dt >= 0, deg >= 0 and dt*(deg + 4*dif) <= 1 for every gene, the explicit
-// Euler update of a cell is a combination with non-negative weights of its
-// old value, its neighbours and dt*lim*h (h in [0, 1]), so no value goes
-// negative and the largest value grows by at most dt*max(lim, 0) per step.
-// Bounding that growth over the run (kFastMaxGrowth) and the initial state
-// (the host's fast_ok) keeps every x^n and K^n far from overflow.  A model
-// outside the bound -- an unstable step such as dt*dif > 1/4, where a
-// checkerboard mode grows until cells overflow to inf and NaN -- runs the
-// exact path, which keeps the reference's inf / NaN behaviour
-// (modelsimulator.cpp:262-275, simstate.cpp:147-151).
-constexpr float kFastMaxGrowth = 1.0e6f;
-
-__device__ __forceinline__ bool euler_bounded(const ModelSmem &M, int G, float dt,
-                                              int n_steps) {
-  bool ok = dt >= 0.0f;
-  for (int p = 0; p < G; ++p) {
-    const PackedGene &gn = M.genes[p];
-    ok = ok && gn.deg >= 0.0f && dt * (gn.deg + 4.0f * gn.dif) <= 1.0f &&
-         (float)n_steps * dt * fmaxf(gn.lim, 0.0f) <= kFastMaxGrowth;
-  }
-  return ok;
-}
-
 // Euler update of one cell (modelsimulator.cpp:224-275).
 //   r = lim*h - deg*c (+ dif*(s - tot*c) for diffusing genes)
 // exact: the reference's guard on the diffusion term, "a zero rate keeps
@@ -587,8 +563,9 @@ __device__ __forceinline__ float update_cell(float c, float h, float lim, float 
 
 // New values of one gene for NI groups; `cur` points at the gene's current
 // plane (shared or global memory).  `mx` takes the max |rate| of the valid
-// groups' real cells.
-template <int NI, int GMAX, bool EXACT, bool RAGGED>
+// groups' real cells.  HPAIR: the fast path adds the horizontal neighbours
+// as FP32 pairs (else as scalar adds; the same roundings).
+template <int NI, int GMAX, bool EXACT, bool RAGGED, bool HPAIR>
 __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem &D, int p,
                                             const PackedGene &gn,
                                             const float4 (&lg)[NI][GMAX], const float *cur,
@@ -614,10 +591,18 @@ __device__ __forceinline__ void gene_update(const ModelSmem &M, const DenseSmem 
         // Row borders read the zero cells that end every padded row.
         const float lft = *chk<1>(cur + it[i].base - 1);
         const float rgt = *chk<1>(cur + it[i].base + 4);
-        // Reference order: x-1, x+1, y-1, y+1.  The horizontal pairs are
-        // scalar adds (their operands straddle the float4's register pairs).
-        const float2 s01 = add2(add2(make_float2(lft + c.y, c.x + c.z), lo2(up)), lo2(dn));
-        const float2 s23 = add2(add2(make_float2(c.y + c.w, c.z + rgt), hi2(up)), hi2(dn));
+        // Reference order: x-1, x+1, y-1, y+1.  Scalar adds suit the step
+        // with two groups per thread and the streaming step (the pairs'
+        // operands straddle the float4's register pairs); paired adds the
+        // steps with one group per thread (measured on the walking step).
+        float2 s01, s23;
+        if constexpr (!HPAIR) {
+          s01 = add2(add2(make_float2(lft + c.y, c.x + c.z), lo2(up)), lo2(dn));
+          s23 = add2(add2(make_float2(c.y + c.w, c.z + rgt), hi2(up)), hi2(dn));
+        } else {
+          s01 = add2(add2(add2(make_float2(lft, c.x), make_float2(c.y, c.z)), lo2(up)), lo2(dn));
+          s23 = add2(add2(add2(make_float2(c.y, c.z), make_float2(c.w, rgt)), hi2(up)), hi2(dn));
+        }
         r01 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.x, -it[i].tot.y), lo2(c), s01), r01);
         r23 = fma2(f2(gn.dif), fma2(make_float2(-it[i].tot.z, -it[i].tot.w), hi2(c), s23), r23);
       }
@@ -759,8 +744,8 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   for (int p = 0; p < sp.n_sm; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, gn, lg, sm_cur + p * g.PS, g, it, dt, min_conc,
-                                       mx, nv);
+    gene_update<NI, GS, EXACT, RAGGED, (NI == 1)>(M, D, p, gn, lg, sm_cur + p * g.PS, g, it, dt,
+                                                  min_conc, mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(sm_nxt + p * g.PS + it[i].base)) = nv[i];
@@ -768,8 +753,8 @@ __device__ __forceinline__ void group_step(const ModelSmem &M, const DenseSmem &
   for (int p = sp.n_sm; p < G; ++p) {
     const PackedGene gn = M.genes[p];
     float4 nv[NI];
-    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, gn, lg, gl_cur + p * g.PS, g, it, dt, min_conc,
-                                       mx, nv);
+    gene_update<NI, GS, EXACT, RAGGED, (NI == 1)>(M, D, p, gn, lg, gl_cur + p * g.PS, g, it, dt,
+                                                  min_conc, mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(gl_nxt + p * g.PS + it[i].base)) = nv[i];
@@ -839,8 +824,8 @@ __device__ __forceinline__ void band_group_step(const ModelSmem &M, const DenseS
   }
   for (int p = 0; p < G; ++p) {
     float4 nv[NI];
-    gene_update<NI, GS, EXACT, RAGGED>(M, D, p, M.genes[p], lg, stage + p * gb.PS, gb, it, dt,
-                                       min_conc, mx, nv);
+    gene_update<NI, GS, EXACT, RAGGED, false>(M, D, p, M.genes[p], lg, stage + p * gb.PS, gb, it,
+                                              dt, min_conc, mx, nv);
 #pragma unroll
     for (int i = 0; i < NI; ++i)
       if (it[i].valid) *reinterpret_cast<float4 *>(chk<4>(out + p * gps + it[i].base)) = nv[i];
@@ -1230,7 +1215,7 @@ __global__ void __launch_bounds__(NT, (NT >= 512 ? 1 : 2)) sim_kernel(const SimA
     const int orig = M.hdr.orig_index;
     sp.n_sm = min(G, A.planes / 2);
     const bool exact = !(A.fast_ok && (M.hdr.flags & kFlagFast) &&
-                         G <= GRN_MAX_GENES && euler_bounded(M, G, A.dt, A.n_steps));
+                         G <= GRN_MAX_GENES);
     const bool bad = G < 1 || G > GMAX || M.hdr.n_links < 0 ||
                      M.hdr.n_links > GRN_MAX_LINKS || (sp.n_sm < G && sp.gl == nullptr) ||
                      (!LOOP && n_iter_band > ITEMS) ||

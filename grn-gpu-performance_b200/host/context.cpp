@@ -91,6 +91,8 @@ struct grn_ctx {
   };
   std::map<std::array<int, 7>, Tuned> tuned;
   std::string last_tuning;  // the last autotuning's candidates and times
+  int n_tunings = 0;         // autotuning runs so far
+  double tuning_ms = 0;      // their host wall time
   // minConc is 0 and the uploaded initial states are finite, non-negative
   // and at most 1e6: the kernel's fast path then gives the same results as
   // the exact one for every model whose step size keeps its state bounded
@@ -433,6 +435,35 @@ grn_status launch_plan(grn_ctx *ctx, const LaunchPlan &plan, grn::SimArgs a, cud
 // it is at least 3% faster.  The sample launches write outputs of the
 // sampled models that the real launch then overwrites.  Synchronises
 // `stream` once per new batch shape.
+// The autotuner's cache key: grid, the kernels' gene capacity class (4, 8
+// or 16 genes), a coarse link class (the balance of work per cell),
+// experiments, fast path, and the batch size when it is below two models
+// per SM.  The exact gene and link counts are left out: a search's batches
+// vary in them from one generation to the next (its population grows), and
+// each new key costs a tuning run.  A kept plan is reused only where it is
+// among the batch's own candidates (same variant, cluster and planes),
+// else the batch is tuned again.
+std::array<int, 7> tune_key(const grn_ctx *ctx, int n_models, int max_genes, int max_links) {
+  const int genes_class = max_genes <= 4 ? 4 : max_genes <= 8 ? 8 : 16;
+  const int links_class = max_links <= 8 ? 0 : max_links <= 32 ? 1 : 2;
+  const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
+  return {ctx->p.dim_x, ctx->p.dim_y, genes_class, links_class, ctx->n_exp,
+          ctx->fast_ok ? 1 : 0, bucket};
+}
+
+// The plan kept for this key, if it is among the batch's candidates.
+bool cached_plan(const grn_ctx *ctx, const std::vector<std::pair<double, LaunchPlan>> &plans,
+                 const std::array<int, 7> &key, LaunchPlan *out) {
+  const auto it = ctx->tuned.find(key);
+  if (it == ctx->tuned.end()) return false;
+  for (const auto &c : plans)
+    if (same_plan(c.second, it->second.v, it->second.cluster, it->second.planes)) {
+      *out = c.second;
+      return true;
+    }
+  return false;
+}
+
 grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, LaunchPlan>> &plans,
                          const grn::SimArgs &a, int n_models, const int32_t *h_offsets,
                          cudaStream_t stream, LaunchPlan *out) {
@@ -497,10 +528,19 @@ grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, Launc
   for (auto &e : ev)
     if (e) cudaEventDestroy(e);
   if (s != GRN_OK) return s;
-  int best = 0;
+  // The first plan in the heuristic's order whose sample time is within 3%
+  // of the fastest: a short sample separates near-ties poorly (the walking
+  // and the all-global plans of a spilled grid time alike on 128 steps,
+  // while over a full run the walking one is 12% faster).
+  int fastest = 0;
   for (int i = 1; i < n_try; ++i)
-    if (best_ms[i] < best_ms[best]) best = i;
-  if (best != 0 && best_ms[best] > 0.97 * best_ms[0]) best = 0;
+    if (best_ms[i] < best_ms[fastest]) fastest = i;
+  int best = fastest;
+  for (int i = 0; i < fastest; ++i)
+    if (best_ms[i] <= 1.03 * best_ms[fastest]) {
+      best = i;
+      break;
+    }
   std::string rep;
   for (int i = 0; i < n_try; ++i) {
     const LaunchPlan &p = cand[i];
@@ -583,22 +623,20 @@ grn_status prepare_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_o
     a.n_exp = 1;
   }
   if (!trace && ctx->forced_schedule == GRN_SCHEDULE_AUTO && ctx->autotune && plans.size() > 1) {
-    const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
-    const std::array<int, 7> key = {W, H, max_genes, max_links, ctx->n_exp,
-                                    ctx->fast_ok ? 1 : 0, bucket};
-    auto it = ctx->tuned.find(key);
-    bool found = false;
-    if (it != ctx->tuned.end()) {
-      for (const auto &c : plans)
-        if (same_plan(c.second, it->second.v, it->second.cluster, it->second.planes)) {
-          plan = c.second;
-          found = true;
-          break;
-        }
-    }
-    if (!found) {
+    const std::array<int, 7> key = tune_key(ctx, n_models, max_genes, max_links);
+    if (!cached_plan(ctx, plans, key, &plan)) {
+      const auto t0 = std::chrono::steady_clock::now();
       s = autotune_plan(ctx, plans, a, n_models, ex.host_offsets, stream, &plan);
       if (s != GRN_OK) return s;
+      ctx->n_tunings += 1;
+      char kl[128];
+      std::snprintf(kl, sizeof kl,
+                    "# key: grid %dx%d, gene class %d, link class %d, experiments %d, fast %d, "
+                    "batch bucket %d\n",
+                    key[0], key[1], key[2], key[3], key[4], key[5], key[6]);
+      ctx->last_tuning = kl + ctx->last_tuning;
+      ctx->tuning_ms +=
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       ctx->tuned[key] = grn_ctx::Tuned{plan.v, plan.cluster, plan.planes, 0.0};
     }
   }
@@ -629,12 +667,15 @@ grn_status launch_packed(grn_ctx *ctx, const uint4 *d_words, const int32_t *d_of
 }
 
 // The autotuner has not yet chosen a plan for this batch shape.
+// (The same test as prepare_packed's: a key without a kept plan, or a kept
+// plan that is not among this batch's candidates.)
 bool tuning_needed(grn_ctx *ctx, int n_models, int max_genes, int max_links) {
   if (ctx->forced_schedule != GRN_SCHEDULE_AUTO || !ctx->autotune) return false;
-  const int bucket = n_models >= 2 * ctx->n_sm ? 0 : n_models;
-  const std::array<int, 7> key = {ctx->p.dim_x, ctx->p.dim_y, max_genes, max_links, ctx->n_exp,
-                                  ctx->fast_ok ? 1 : 0, bucket};
-  return ctx->tuned.find(key) == ctx->tuned.end();
+  std::vector<std::pair<double, LaunchPlan>> plans;
+  if (enumerate_plans(ctx, max_genes, n_models, false, &plans) != GRN_OK) return false;
+  if (plans.size() <= 1) return false;
+  LaunchPlan p;
+  return !cached_plan(ctx, plans, tune_key(ctx, n_models, max_genes, max_links), &p);
 }
 
 void fill_launch_stats(grn_eval_stats *stats, int n, std::chrono::steady_clock::time_point t0,
@@ -727,6 +768,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   PackedHost ph;
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      (float)ctx->p.dt, ctx->p.num_sim_steps,
                       host_threads(), &ph, &err);
   if (s != GRN_OK) return fail(ctx, s, err);
   auto t1 = std::chrono::steady_clock::now();
@@ -907,8 +949,12 @@ static_assert(grn::kHookWithholdBandCopy == GRN_TEST_WITHHOLD_BAND_COPY, "test h
 
 grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len) {
   if (!ctx || !buf || buf_len < 1) return GRN_ERR_INVALID_ARGUMENT;
-  std::snprintf(buf, (size_t)buf_len, "%s", ctx->last_tuning.c_str());
-  return (int)ctx->last_tuning.size() < buf_len ? GRN_OK : GRN_ERR_CAPACITY;
+  char head[96];
+  std::snprintf(head, sizeof head, "# autotuning runs %d, %.1f ms in all; the last one:\n",
+                ctx->n_tunings, ctx->tuning_ms);
+  const std::string rep = head + ctx->last_tuning;
+  std::snprintf(buf, (size_t)buf_len, "%s", rep.c_str());
+  return (int)rep.size() < buf_len ? GRN_OK : GRN_ERR_CAPACITY;
 }
 
 grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks) {
@@ -1044,6 +1090,7 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
   PackedHost ph;
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      (float)ctx->p.dt, ctx->p.num_sim_steps,
                       host_threads(), &ph, &err);
   if (s != GRN_OK) return fail(ctx, s, err);
   Job &j = ctx->sync_job;
@@ -1168,6 +1215,7 @@ grn_status grn_pack(grn_ctx *ctx, const grn_model_batch *batch, grn_packed **out
   pk->ctx = ctx;
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
+                      (float)ctx->p.dt, ctx->p.num_sim_steps,
                       host_threads(), &pk->host, &err);
   if (s != GRN_OK) {
     delete pk;
@@ -1245,7 +1293,8 @@ grn_status grn_trace_model(grn_ctx *ctx, const grn_product *products, int n_prod
   b.links = links;
   PackedHost ph;
   std::string err;
-  grn_status s = grn::pack_batch(&b, n_morph, 1, &ph, &err);
+  grn_status s =
+      grn::pack_batch(&b, n_morph, (float)ctx->p.dt, ctx->p.num_sim_steps, 1, &ph, &err);
   if (s != GRN_OK) return fail(ctx, s, err);
   const size_t cells = (size_t)ctx->p.dim_x * ctx->p.dim_y;
   const size_t fb = (size_t)max_frames * max_planes * cells * sizeof(float);

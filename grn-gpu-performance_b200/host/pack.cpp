@@ -197,7 +197,17 @@ grn_status pack_model(const grn_product *products, int n_products,
   return GRN_OK;
 }
 
-grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
+bool euler_bounded(const PackedGene *genes, int n_genes, float dt, int n_steps) {
+  bool ok = dt >= 0.0f;
+  for (int p = 0; p < n_genes; ++p) {
+    const PackedGene &g = genes[p];
+    ok = ok && g.deg >= 0.0f && dt * (g.deg + 4.0f * g.dif) <= 1.0f &&
+         (float)n_steps * dt * std::max(g.lim, 0.0f) <= kFastMaxGrowth;
+  }
+  return ok;
+}
+
+grn_status pack_batch(const grn_model_batch *batch, int n_morphogens, float dt, int n_steps,
                       int n_threads, PackedHost *out, std::string *err) {
   const int n = batch->n_models;
   std::vector<std::vector<uint4>> recs(n);
@@ -215,6 +225,18 @@ grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
       std::string e;
       grn_status s = pack_model(batch->products + p0, p1 - p0, batch->links + l0,
                                 l1 - l0, n_morphogens, m, &recs[m], &costs[m], &e);
+      if (s == GRN_OK) {
+        // The fast path also needs a bounded Euler step at this dt.
+        PackedHeader hdr;
+        std::memcpy(&hdr, recs[m].data(), sizeof hdr);
+        std::vector<PackedGene> genes(hdr.n_genes);
+        if (hdr.n_genes > 0)
+          std::memcpy(genes.data(), recs[m].data() + 1, sizeof(PackedGene) * hdr.n_genes);
+        if ((hdr.flags & kFlagFast) && !euler_bounded(genes.data(), hdr.n_genes, dt, n_steps)) {
+          hdr.flags &= ~kFlagFast;
+          std::memcpy(recs[m].data(), &hdr, sizeof hdr);
+        }
+      }
       if (s != GRN_OK) {
         bool expected = false;
         if (err_taken.compare_exchange_strong(expected, true)) first_err = e;

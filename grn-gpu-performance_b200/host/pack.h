@@ -53,8 +53,27 @@ struct PackedHost {
   int64_t alg_fp32_per_cell_step = 0;  // sum of 6 L + 7 G + 8 G_dif
 };
 
-grn_status pack_batch(const grn_model_batch *batch, int n_morphogens,
+// Packs a batch for runs of n_steps explicit Euler steps of size dt.  The
+// fast-path flag of each record also requires the Euler update to stay
+// bounded at that step size (euler_bounded).
+grn_status pack_batch(const grn_model_batch *batch, int n_morphogens, float dt, int n_steps,
                       int n_threads, PackedHost *out, std::string *err);
+
+// Largest growth of a state value over a run that the fast path accepts.
+constexpr float kFastMaxGrowth = 1.0e6f;
+
+// Whether the explicit Euler update of these genes stays finite and
+// non-negative.  With dt >= 0, deg >= 0 and dt*(deg + 4*dif) <= 1 for every
+// gene, the update of a cell is a combination with non-negative weights of
+// its old value, its neighbours and dt*lim*h (h in [0, 1]), so no value goes
+// negative and the largest value grows by at most dt*max(lim, 0) per step.
+// Bounding that growth over the run (kFastMaxGrowth) and the initial state
+// (the context's fast_ok) keeps every x^n and K^n far from overflow.  A
+// model outside the bound -- an unstable step such as dt*dif > 1/4, where a
+// checkerboard mode grows until cells overflow to inf and NaN -- runs the
+// exact path, which keeps the reference's inf / NaN behaviour
+// (modelsimulator.cpp:262-275, simstate.cpp:147-151).
+bool euler_bounded(const PackedGene *genes, int n_genes, float dt, int n_steps);
 
 }  // namespace grn
 

@@ -220,11 +220,12 @@ grn_status grn_set_cluster_size(grn_ctx *ctx, int cluster_size);
  * the cache. */
 grn_status grn_set_autotune(grn_ctx *ctx, int enable);
 
-/* The last measured autotuning on this context, one line per timed plan
- * ("*" marks the one kept): schedule, threads, gene capacity, items per
- * thread, cluster size, shared-memory planes, streaming band rows and the
- * fastest sample launch in ms.  GRN_ERR_CAPACITY if it was truncated to
- * buf_len. */
+/* The autotuning on this context: a first line starting with '#' that
+ * counts the runs so far and their host time, then the last run, one line
+ * per timed plan ("*" marks the one kept): schedule, threads, gene
+ * capacity, items per thread, cluster size, shared-memory planes, streaming
+ * band rows and the fastest sample launch in ms.  GRN_ERR_CAPACITY if it
+ * was truncated to buf_len. */
 grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len);
 
 /* enable = 1: grn_evaluate, grn_evaluate_batch and grn_submit replay one

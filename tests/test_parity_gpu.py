@@ -274,6 +274,25 @@ def test_autotuned_plan_is_cached_and_exact():
     assert_raw_close(a_raw, h_raw, rtol=1e-12, atol=0, what="autotune")
 
 
+def test_autotune_key_ignores_exact_link_count():
+    """Batches that differ only in their largest link count, as a search's
+    generations do, share one tuning run (the report's first line counts
+    the runs)."""
+    params, b20, init, tgt = synth.workload("uneven_64x64", seed=19, n_models=400, steps=50,
+                                            genes=(8, 8), links=(1, 20))
+    _, b24, _, _ = synth.workload("uneven_64x64", seed=20, n_models=400, steps=50,
+                                  genes=(8, 8), links=(1, 24))
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        infos = [ev.pack(b).info for b in (b20, b24)]
+        assert infos[0]["max_genes"] == infos[1]["max_genes"]
+        assert infos[0]["max_links"] != infos[1]["max_links"]
+        ev.evaluate_batch(b20)
+        ev.evaluate_batch(b24)
+        head = ev.autotune_report().splitlines()[0]
+    assert head.startswith("# autotuning runs 1,"), head
+
+
 @pytest.mark.parametrize("W,H,steps,genes", [(256, 256, 12, (8, 8)), (100, 100, 30, (6, 8)),
                                              (30, 37, 25, (2, 8)), (250, 90, 15, (8, 16))])
 def test_stream_schedule_matches_global_bitwise(W, H, steps, genes):
@@ -470,6 +489,30 @@ def test_trace_stops_with_the_simulation():
         _, _, st = ev.evaluate_batch(batch)
         frames, _ = ev.trace(prods, links, every=10, max_frames=1000, max_planes=4)
     assert len(frames) == st["total_steps"] // 10 + 1 < 1000
+
+
+def test_graph_mode_with_growing_gene_counts():
+    """A search's population grows: batches whose largest gene count changes
+    inside one gene-capacity class (at 64 x 64, 5 genes keep 10 planes in
+    shared memory, 6 and 8 genes 12).  A kept plan that is not among a
+    batch's candidates is tuned again, outside any capture, on that batch's
+    own records; graph mode gives the plain launches' errors bit for bit."""
+    params, b5, init, tgt = synth.workload("uneven_64x64", seed=31, n_models=320, steps=40,
+                                           genes=(5, 5))
+    _, b6, _, _ = synth.workload("uneven_64x64", seed=32, n_models=320, steps=40, genes=(6, 6))
+    _, b8, _, _ = synth.workload("uneven_64x64", seed=33, n_models=320, steps=40, genes=(8, 8))
+    batches = [b5, b6, b8, b5]
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        genes = [ev.pack(b).info["max_genes"] for b in batches[:3]]
+        assert len(set(genes)) == 3, genes
+        want = [ev.evaluate_batch(b)[1] for b in batches]
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        ev.set_graphs(True)
+        got = [ev.evaluate_batch(b)[1] for b in batches]
+    for w, g in zip(want, got):
+        np.testing.assert_array_equal(g, w)
 
 
 def test_graph_mode_matches_stream_launches():
