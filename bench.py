@@ -197,8 +197,11 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     wl = synth.WORKLOADS[args.workload]
     vals = []
+    # Each step is a bounded sample; the whole run stays near 150 s of CPU
+    # time whatever --steps / --warmup ask for (2 s per sample at least).
+    budget = max(2.0, min(args.ref_budget, 150.0 / max(1, args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(args.workload, seed=i, budget_s=args.ref_budget, threads=threads)
+        cb = cpu_baseline(args.workload, seed=i, budget_s=budget, threads=threads)
         if i >= args.warmup:
             vals.append(cb)
     value = statistics.mean(v["value"] for v in vals)
