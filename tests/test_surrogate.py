@@ -351,3 +351,28 @@ def test_short_run_screen_fades_as_population_converges(built_libs):
     assert rho[:3].mean() > 0.4          # ranks like the full run at first
     assert rho[-5:].mean() < 0.1         # and at chance once the population converged
     assert np.nanmean(rec) < 0.25        # no better than keeping children at random
+
+
+@pytest.mark.gpu
+def test_surrogate_tiny_and_ragged_batches(built_libs):
+    """Batches smaller than one 128-row tile and weight-gradient GEMMs whose
+    reduction (the batch) is shorter than one 64-wide slice: the tensor maps
+    zero-fill past the edges.  Predictions and gradients on the tcgen05 path
+    against the BF16-emulating FP64 MLP (tolerances as in the gradient
+    check)."""
+    rng = np.random.default_rng(9)
+    s = grn.Surrogate(seed=19)
+    p = s.params().astype(np.float64)
+    for n in (1, 5, 7, 64, 129):
+        x = rng.normal(size=(n, 128)).astype(np.float32)
+        t = (rng.normal(size=n) - 1).astype(np.float32)
+        y = s.predict(x)
+        y_ref, _ = mlp_ref.forward(p, x, emulate_bf16=True)
+        assert np.linalg.norm(y - y_ref) <= 2e-3 * np.linalg.norm(y_ref), n
+        loss, g = s.gradients(x, t)
+        ref_loss, ref_g = mlp_ref.loss_and_grads(p, x, t, emulate_bf16=True)
+        assert abs(loss - ref_loss) <= 1e-4 * ref_loss, n
+        gb, rb = _blocks(g), _blocks(ref_g)
+        for name, _ in mlp_ref.SHAPES:
+            assert np.linalg.norm(gb[name] - rb[name]) <= 5e-3 * np.linalg.norm(rb[name]) + 1e-7, \
+                (n, name)
