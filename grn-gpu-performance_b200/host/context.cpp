@@ -25,6 +25,7 @@
 #include "../../include/grn_gpu.h"
 #include "../csrc/grn_sim.h"
 #include "pack.h"
+#include "trace.h"
 
 namespace {
 
@@ -467,6 +468,7 @@ bool cached_plan(const grn_ctx *ctx, const std::vector<std::pair<double, LaunchP
 grn_status autotune_plan(grn_ctx *ctx, const std::vector<std::pair<double, LaunchPlan>> &plans,
                          const grn::SimArgs &a, int n_models, const int32_t *h_offsets,
                          cudaStream_t stream, LaunchPlan *out) {
+  grn::TraceRange trace_range("grn autotune");
   grn::SimArgs t = a;
   // About 2^29 cell-updates per sample launch: up to 8 models per SM (so
   // that, as in the full batch, the slowest block's last model is a small
@@ -1065,6 +1067,7 @@ grn_status grn_set_experiments_rgb(grn_ctx *ctx, int n_experiments, const uint32
 
 grn_status grn_evaluate_batch(grn_ctx *ctx, const grn_model_batch *batch, const double *max_error,
                               double *error_out, double *raw_error_out, grn_eval_stats *stats) {
+  grn::TraceRange trace_range("grn_evaluate_batch");
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
   if (!error_out && !raw_error_out)
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -1078,6 +1081,7 @@ grn_status grn_evaluate_batch(grn_ctx *ctx, const grn_model_batch *batch, const 
 
 grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const double *max_error,
                                double *raw_error_out, float *states_out, int max_planes) {
+  grn::TraceRange trace_range("grn_evaluate_states");
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
   grn_status s = check_batch(ctx, batch);
   if (s != GRN_OK) return s;
@@ -1154,6 +1158,7 @@ grn_status grn_evaluate(grn_ctx *ctx, const grn_product *products, int n_product
 
 grn_status grn_submit(grn_ctx *ctx, int tag, const grn_model_batch *batch, const double *max_error,
                       double *error_out, double *raw_error_out) {
+  grn::TraceRange trace_range("grn_submit");
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
   if (!error_out && !raw_error_out)
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "no output buffer");
@@ -1180,6 +1185,7 @@ grn_status grn_submit(grn_ctx *ctx, int tag, const grn_model_batch *batch, const
 }
 
 grn_status grn_wait_any(grn_ctx *ctx, int timeout_ms, int *tag_out) {
+  grn::TraceRange trace_range("grn_wait_any");
   if (!ctx || !tag_out) return GRN_ERR_INVALID_ARGUMENT;
   if (ctx->pending.empty()) return fail(ctx, GRN_ERR_NOT_FOUND, "nothing submitted");
   cudaSetDevice(ctx->device);
@@ -1205,6 +1211,7 @@ grn_status grn_wait_any(grn_ctx *ctx, int timeout_ms, int *tag_out) {
 }
 
 grn_status grn_pack(grn_ctx *ctx, const grn_model_batch *batch, grn_packed **out) {
+  grn::TraceRange trace_range("grn_pack");
   if (!ctx || !out) return GRN_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   grn_status s = check_batch(ctx, batch);
@@ -1348,6 +1355,7 @@ grn_status grn_trace_model(grn_ctx *ctx, const grn_product *products, int n_prod
 
 grn_status grn_run_packed(grn_ctx *ctx, const grn_packed *pk, const double *d_max_error,
                           double *d_raw_error, int32_t *d_steps, void *cuda_stream) {
+  grn::TraceRange trace_range("grn_run_packed");
   if (!ctx || !pk || pk->ctx != ctx) return GRN_ERR_INVALID_ARGUMENT;
   if (pk->host.n_models > 0 && (!d_max_error || !d_raw_error))
     return fail(ctx, GRN_ERR_INVALID_ARGUMENT, "null device pointer");

@@ -12,6 +12,7 @@
 // selects and, every migration_period generations, random deme pairs mix.
 
 #include "evolution.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <chrono>
@@ -394,6 +395,7 @@ struct FlatBatch {
 // unrounded errors when the GPU evaluator is used, else the rounded ones.
 grn_status evaluate_all(grn_evolution *evo, std::vector<Individual *> &inds,
                         std::vector<double> *raw_out) {
+  grn::TraceRange trace_range("grn evaluate children");
   FlatBatch fb(inds);
   std::vector<double> max_err, err(inds.size()), raw(inds.size());
   for (Individual *ind : inds) max_err.push_back(ind->parent_error);
@@ -454,6 +456,7 @@ bool same_key(const std::vector<double> &a, const std::vector<double> &b) {
 // biased towards children that beat their parents.
 grn_status feed_surrogate(grn_evolution *evo, const std::vector<Individual *> &inds,
                           const std::vector<double> &raw, grn_generation_stats *st) {
+  grn::TraceRange trace_range("grn surrogate training");
   std::vector<Individual *> keep;
   std::vector<float> target;
   for (size_t i = 0; i < inds.size(); ++i) {
@@ -899,6 +902,7 @@ grn_status grn_evolution_set_pipeline(grn_evolution *evo, int enable) {
 }
 
 grn_status grn_evolution_step(grn_evolution *evo, grn_generation_stats *stats) {
+  grn::TraceRange trace_range("grn_evolution_step");
   if (!evo) return GRN_ERR_INVALID_ARGUMENT;
   grn_generation_stats st{};
   if (evo->pipelined && evo->generation >= 0) {

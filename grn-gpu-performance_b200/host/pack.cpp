@@ -1,5 +1,6 @@
 // pack.cpp -- host compiler from genome-form models to packed programs.
 #include "pack.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <atomic>
@@ -209,6 +210,7 @@ bool euler_bounded(const PackedGene *genes, int n_genes, float dt, int n_steps) 
 
 grn_status pack_batch(const grn_model_batch *batch, int n_morphogens, float dt, int n_steps,
                       int n_threads, PackedHost *out, std::string *err) {
+  grn::TraceRange trace_range("grn pack_batch");
   const int n = batch->n_models;
   std::vector<std::vector<uint4>> recs(n);
   std::vector<ModelCost> costs(n);

@@ -18,6 +18,7 @@
 #include "../../include/grn_gpu.h"
 #include "../csrc/grn_mlp.h"
 #include "pack.h"
+#include "trace.h"
 
 namespace {
 
@@ -405,6 +406,7 @@ int grn_surrogate_data_count(const grn_surrogate *s) { return s ? s->count : 0; 
 
 grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, float lr,
                                double *mean_loss) {
+  grn::TraceRange trace_range("grn_surrogate_train");
   if (!s || epochs < 0 || batch_size < 1 || batch_size > s->bmax || !(lr > 0))
     return GRN_ERR_INVALID_ARGUMENT;
   if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
@@ -426,6 +428,7 @@ grn_status grn_surrogate_train(grn_surrogate *s, int epochs, int batch_size, flo
 
 grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batch_size, float lr,
                                        double *mean_loss) {
+  grn::TraceRange trace_range("grn_surrogate_train_batches");
   if (!s || n_batches < 0 || batch_size < 1 || batch_size > s->bmax || !(lr > 0))
     return GRN_ERR_INVALID_ARGUMENT;
   if (s->count == 0) return GRN_ERR_INVALID_ARGUMENT;
@@ -440,6 +443,7 @@ grn_status grn_surrogate_train_batches(grn_surrogate *s, int n_batches, int batc
 }
 
 grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n, float *out) {
+  grn::TraceRange trace_range("grn_surrogate_predict");
   if (!s || n < 0 || (n > 0 && (!features || !out))) return GRN_ERR_INVALID_ARGUMENT;
   cudaSetDevice(s->device);
   for (int i = 0; i < n; i += s->bmax) {
