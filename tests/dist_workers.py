@@ -119,3 +119,30 @@ def cuda_one_rank(rank, world, port, root, out):
              raw_p=raw_p, best_sharded=best_sharded, best_plain=best_plain)
     dist.barrier()
     dist.destroy_process_group()
+
+
+def sharded_rank_dies(rank, world, port, root, out):
+    """Rank 1 dies between steps (after a completed gather, before the
+    next); rank 0's next gather must end in an error, not wait for good."""
+    import datetime
+    import time
+    dist = _setup(root, rank, world, port)
+    import numpy as np
+    import synth
+    import sharded
+    params, batch, init, tgt = synth.workload("small_32x32", seed=22, n_models=9, steps=20,
+                                              W=8, H=8)
+    ev = OracleEvaluator(params, init, tgt)
+    sh = sharded.ShardedEvaluator(ev, params["n_input_morphogens"] +
+                                  params["n_target_morphogens"])
+    err, raw, _ = sh.evaluate_batch(batch)  # one step that both ranks finish
+    if rank == 1:
+        os._exit(3)  # no clean-up: the process is gone
+    t0 = time.monotonic()
+    try:
+        sh.evaluate_batch(batch)
+        outcome = "returned"
+    except Exception as e:  # the backend's error for a lost peer
+        outcome = "raised " + type(e).__name__
+    np.savez(os.path.join(out, "rank0.npz"), outcome=outcome, seconds=time.monotonic() - t0,
+             first=raw)

@@ -75,6 +75,27 @@ def test_island_shards_migrate_across_ranks(built_libs, tmp_path):
             assert np.array_equal(p3, p2) and np.array_equal(l3, l2) and err3 == err2
 
 
+def test_lost_rank_ends_the_next_gather_with_an_error(built_libs, tmp_path):
+    """Failure detection on the host: a rank that dies between steps (with
+    nothing of its own in flight) makes the survivor's next collective
+    raise within the process group's timeout instead of hanging."""
+    ctx = mp.start_processes(dist_workers.sharded_rank_dies,
+                             args=(2, _port(), ROOT, str(tmp_path)), nprocs=2, join=False,
+                             start_method="spawn")
+    deadline = 90.0
+    for p in ctx.processes:
+        p.join(deadline)
+    alive = [p for p in ctx.processes if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a rank did not finish"
+    assert [p.exitcode for p in ctx.processes] == [0, 3]
+    r = np.load(tmp_path / "rank0.npz")
+    print("survivor:", str(r["outcome"]), "after %.1f s" % float(r["seconds"]))
+    assert str(r["outcome"]).startswith("raised"), str(r["outcome"])
+    assert float(r["seconds"]) < 70.0
+
+
 @pytest.mark.gpu
 def test_sharding_runs_over_the_cuda_evaluator(built_libs, tmp_path):
     """The sharding code over the real CUDA evaluator on a one-rank NCCL
