@@ -160,6 +160,8 @@ _SIGNATURES = {
                          ctypes.POINTER(_I)], _I),
     "grn_evolution_set_individual": ([_P, _I, _I, _P, _I, _P, _I, _D], _I),
     "grn_evolution_set_generation": ([_P, _I], _I),
+    "grn_evolution_checkpoint": ([_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], _I),
+    "grn_evolution_restore": ([_P, _P, ctypes.c_size_t], _I),
     "grn_evolution_set_pipeline": ([_P, _I], _I),
     "grn_surrogate_create": ([_I, ctypes.c_uint64, _I, ctypes.POINTER(_P)], _I),
     "grn_surrogate_destroy": ([_P], _I),
@@ -580,6 +582,18 @@ class Evolution:
 
     def set_generation(self, generation):
         _check(self.lib.grn_evolution_set_generation(self.handle, generation))
+
+    def checkpoint(self):
+        """The search's exact state as bytes (grn_evolution_checkpoint)."""
+        n = ctypes.c_size_t()
+        _check(self.lib.grn_evolution_checkpoint(self.handle, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(self.lib.grn_evolution_checkpoint(self.handle, buf, n.value, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def restore(self, state):
+        """Continues from a checkpoint of a search with the same parameters."""
+        _check(self.lib.grn_evolution_restore(self.handle, state, len(state)))
 
     def set_skip_clones(self, enable=True):
         _check(self.lib.grn_evolution_set_skip_clones(self.handle, int(bool(enable))))

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <sstream>
 #include <string>
 #include <thread>
 
@@ -1115,6 +1116,169 @@ grn_status grn_evolution_set_generation(grn_evolution *evo, int generation) {
         evo->last_error = "an individual has no model";
         return GRN_ERR_MODEL;
       }
+  evo->generation = generation;
+  return GRN_OK;
+}
+
+}  // extern "C"
+
+// ---- checkpoint ----------------------------------------------------------
+//
+// Layout (host byte order, this library's struct layouts): magic, version,
+// the search's shape, generation, the search RNG, then per deme its RNG,
+// label source, pairing permutation and population (error, parent error,
+// complexity, products, links).  RNG states go through the standard
+// library's text form of std::mt19937_64.
+
+namespace {
+
+constexpr char kCheckpointMagic[8] = {'G', 'R', 'N', 'E', 'V', 'O', 'C', 'K'};
+constexpr uint32_t kCheckpointVersion = 1;
+
+struct Writer {
+  std::string out;
+  template <class T>
+  void pod(const T &v) {
+    out.append(reinterpret_cast<const char *>(&v), sizeof v);
+  }
+  void str(const std::string &v) {
+    pod((uint64_t)v.size());
+    out += v;
+  }
+  template <class T>
+  void vec(const std::vector<T> &v) {
+    pod((uint64_t)v.size());
+    if (!v.empty()) out.append(reinterpret_cast<const char *>(v.data()), sizeof(T) * v.size());
+  }
+};
+
+struct Reader {
+  const char *p, *end;
+  template <class T>
+  bool pod(T *v) {
+    if ((size_t)(end - p) < sizeof *v) return false;
+    std::memcpy(v, p, sizeof *v);
+    p += sizeof *v;
+    return true;
+  }
+  bool str(std::string *v, uint64_t max_len) {
+    uint64_t n = 0;
+    if (!pod(&n) || n > max_len || (uint64_t)(end - p) < n) return false;
+    v->assign(p, (size_t)n);
+    p += n;
+    return true;
+  }
+  template <class T>
+  bool vec(std::vector<T> *v, uint64_t max_n) {
+    uint64_t n = 0;
+    if (!pod(&n) || n > max_n || (uint64_t)(end - p) / sizeof(T) < n) return false;
+    v->resize((size_t)n);
+    if (n) std::memcpy(v->data(), p, sizeof(T) * n);
+    p += sizeof(T) * n;
+    return true;
+  }
+};
+
+std::string rng_text(const grn::Rng &r) {
+  std::ostringstream o;
+  r.save(o);
+  return o.str();
+}
+
+bool rng_from_text(const std::string &t, grn::Rng *r) {
+  std::istringstream i(t);
+  return r->load(i);
+}
+
+}  // namespace
+
+extern "C" {
+
+grn_status grn_evolution_checkpoint(const grn_evolution *evo, void *buf, size_t cap,
+                                    size_t *size) {
+  if (!evo || !size) return GRN_ERR_INVALID_ARGUMENT;
+  if (evo->primed) return GRN_ERR_INVALID_ARGUMENT;  // children in flight (pipelined)
+  Writer w;
+  w.out.append(kCheckpointMagic, sizeof kCheckpointMagic);
+  w.pod(kCheckpointVersion);
+  w.pod(evo->p.n_demes);
+  w.pod(evo->p.deme_size);
+  w.pod(evo->ops.n_morph);
+  w.pod(evo->p.n_max_products);
+  w.pod(evo->p.n_max_links);
+  w.pod(evo->generation);
+  w.str(rng_text(evo->search_rng));
+  for (const Deme &d : evo->demes) {
+    w.str(rng_text(d.rng));
+    w.pod(d.labels.next);
+    w.pod(d.labels.stride);
+    w.vec(d.perm);
+    w.pod((uint64_t)d.pop.size());
+    for (const Individual &ind : d.pop) {
+      w.pod(ind.error);
+      w.pod(ind.parent_error);
+      w.pod(ind.complexity);
+      w.vec(ind.model.prods);
+      w.vec(ind.model.links);
+    }
+  }
+  *size = w.out.size();
+  if (!buf) return GRN_OK;
+  if (cap < w.out.size()) return GRN_ERR_CAPACITY;
+  std::memcpy(buf, w.out.data(), w.out.size());
+  return GRN_OK;
+}
+
+grn_status grn_evolution_restore(grn_evolution *evo, const void *buf, size_t size) {
+  if (!evo || !buf) return GRN_ERR_INVALID_ARGUMENT;
+  Reader r{static_cast<const char *>(buf), static_cast<const char *>(buf) + size};
+  auto bad = [&](const char *why) {
+    evo->last_error = std::string("checkpoint: ") + why;
+    return GRN_ERR_INVALID_ARGUMENT;
+  };
+  char magic[sizeof kCheckpointMagic];
+  uint32_t version = 0;
+  if (!r.pod(&magic) || std::memcmp(magic, kCheckpointMagic, sizeof magic) != 0 ||
+      !r.pod(&version) || version != kCheckpointVersion)
+    return bad("not a checkpoint of this version");
+  int32_t n_demes = 0, deme_size = 0, n_max_products = 0, n_max_links = 0;
+  int n_morph = 0, generation = 0;
+  if (!r.pod(&n_demes) || !r.pod(&deme_size) || !r.pod(&n_morph) || !r.pod(&n_max_products) ||
+      !r.pod(&n_max_links) || !r.pod(&generation))
+    return bad("truncated");
+  if (n_demes != evo->p.n_demes || deme_size != evo->p.deme_size ||
+      n_morph != evo->ops.n_morph || n_max_products != evo->p.n_max_products ||
+      n_max_links != evo->p.n_max_links)
+    return bad("the search's shape differs");
+  // Parse everything before changing the search.
+  constexpr uint64_t kMaxText = 1 << 16, kMaxItems = 1 << 24;
+  std::string text;
+  grn::Rng search_rng{0};
+  if (!r.str(&text, kMaxText) || !rng_from_text(text, &search_rng)) return bad("search RNG");
+  std::vector<Deme> demes(evo->demes.size());
+  for (Deme &d : demes) {
+    uint64_t n_pop = 0;
+    if (!r.str(&text, kMaxText) || !rng_from_text(text, &d.rng) || !r.pod(&d.labels.next) ||
+        !r.pod(&d.labels.stride) || !r.vec(&d.perm, kMaxItems) || !r.pod(&n_pop) ||
+        n_pop != (uint64_t)deme_size)
+      return bad("deme state");
+    d.pop.resize((size_t)n_pop);
+    for (Individual &ind : d.pop) {
+      if (!r.pod(&ind.error) || !r.pod(&ind.parent_error) || !r.pod(&ind.complexity) ||
+          !r.vec(&ind.model.prods, kMaxItems) || !r.vec(&ind.model.links, kMaxItems))
+        return bad("individual");
+    }
+    for (int v : d.perm)
+      if (v < 0 || v >= deme_size) return bad("pairing order");
+    if (generation >= 0)
+      for (const Individual &ind : d.pop)
+        if (ind.model.prods.empty()) return bad("an individual has no model");
+  }
+  if (r.p != r.end) return bad("trailing bytes");
+  const grn_status ds = drain(evo);
+  if (ds != GRN_OK) return ds;
+  evo->search_rng = search_rng;
+  evo->demes.swap(demes);
   evo->generation = generation;
   return GRN_OK;
 }

@@ -9,6 +9,8 @@
 
 #include <stdint.h>
 
+#include <istream>
+#include <ostream>
 #include <random>
 #include <vector>
 
@@ -27,6 +29,14 @@ class Rng {
   int rand1000() { return std::uniform_int_distribution<int>(0, 999)(g_); }
   double rand01() { return std::uniform_real_distribution<double>(0.0, 1.0)(g_); }
   double rand15() { return std::uniform_real_distribution<double>(1.0, 5.0)(g_); }
+  // The generator's state in the standard library's text form.
+  void save(std::ostream &o) const { o << g_; }
+  bool load(std::istream &i) {
+    std::mt19937_64 g;
+    if (!(i >> g)) return false;
+    g_ = g;
+    return true;
+  }
   template <class T>
   void shuffle(std::vector<T> &v) {  // Durstenfeld, as MathAlgo::shuffle
     for (int i = (int)v.size() - 1; i > 0; --i) {

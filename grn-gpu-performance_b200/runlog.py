@@ -25,6 +25,8 @@ CREATE TABLE IF NOT EXISTS Generation (
   MinComp INTEGER, MeanComp REAL, MaxComp INTEGER, BestComp INTEGER);
 CREATE TABLE IF NOT EXISTS GenerationIndividual (
   Generation INTEGER NOT NULL, Individual INTEGER NOT NULL, Position INTEGER NOT NULL);
+CREATE TABLE IF NOT EXISTS SearchCheckpoint (
+  Ind INTEGER PRIMARY KEY, State BLOB NOT NULL);
 """
 
 
@@ -42,9 +44,13 @@ class RunLog:
         self.db.commit()
         self.db.close()
 
-    def record_generation(self, evo, n_demes, deme_size, generation, time_s=0.0):
+    def record_generation(self, evo, n_demes, deme_size, generation, time_s=0.0,
+                          checkpoint=False):
         """One Generation row per deme (its error and complexity statistics,
-        Generation::submit's values) plus its individuals."""
+        Generation::submit's values) plus its individuals; with `checkpoint`
+        also the search's exact state (grn_evolution_checkpoint, a table the
+        reference does not have), from which resume continues the run as it
+        would have gone on."""
         cur = self.db.cursor()
         for d in range(n_demes):
             inds = [evo.individual(d, i) for i in range(deme_size)]
@@ -64,6 +70,9 @@ class RunLog:
                     (grn.format_model(prods, links, self.precision), int(comp), float(err), 0.0))
                 cur.execute("INSERT INTO GenerationIndividual VALUES (?,?,?)",
                             (gen_id, cur.lastrowid, pos))
+        if checkpoint:
+            cur.execute("INSERT OR REPLACE INTO SearchCheckpoint VALUES (?,?)",
+                        (generation, sqlite3.Binary(evo.checkpoint())))
         self.db.commit()
 
     def generations(self):
@@ -85,10 +94,17 @@ class RunLog:
         return pop
 
     def resume(self, evo, generation):
-        """Loads a recorded generation into `evo` (same deme count and size):
-        the populations and their errors.  The search's random state is not
-        part of the record, so the continuation differs from the original
-        run's."""
+        """Loads a recorded generation into `evo` (same deme count and size).
+        Where the generation was recorded with its checkpoint, the search
+        continues exactly as the recorded run did (given a deterministic
+        evaluator).  Otherwise only the populations and their errors load,
+        and the search's random state starts afresh, so the continuation
+        differs from the original run's."""
+        row = self.db.execute("SELECT State FROM SearchCheckpoint WHERE Ind = ?",
+                              (generation,)).fetchone()
+        if row is not None:
+            evo.restore(bytes(row[0]))
+            return
         for deme, inds in self.load_population(generation).items():
             for i, (prods, links, err) in enumerate(inds):
                 evo.set_individual(deme, i, prods, links, err)

@@ -529,6 +529,24 @@ grn_status grn_evolution_set_pipeline(grn_evolution *evo, int enable);
  * them (instead of creating random populations) as generation
  * `generation` + 1.  GRN_ERR_MODEL if an individual has no model. */
 grn_status grn_evolution_set_generation(grn_evolution *evo, int generation);
+/* Checkpoint of a search as an opaque byte string: its generation, every
+ * deme's population (models, errors, complexities), pairing order, random
+ * state and label counter, and the search's own random state (the
+ * reference's Search reload, Src/Search/search.cpp:382-434, restores
+ * populations only).  grn_evolution_restore into a search created with the
+ * same parameters continues exactly as the checkpointed search would have,
+ * given a deterministic evaluator.  An attached surrogate is not part of the
+ * checkpoint (save it with grn_surrogate_params).
+ * grn_evolution_checkpoint sets *size to the byte count and writes the bytes
+ * when buf is not NULL (GRN_ERR_CAPACITY if cap is smaller).  A pipelined
+ * search with children in flight cannot be checkpointed
+ * (GRN_ERR_INVALID_ARGUMENT): switch pipelining off first.
+ * grn_evolution_restore checks the search's shape and the bytes' integrity
+ * (GRN_ERR_INVALID_ARGUMENT, the search unchanged) and drops children in
+ * flight. */
+grn_status grn_evolution_checkpoint(const grn_evolution *evo, void *buf, size_t cap,
+                                    size_t *size);
+grn_status grn_evolution_restore(grn_evolution *evo, const void *buf, size_t size);
 grn_status grn_evolution_best(const grn_evolution *evo, int *deme, int *index);
 grn_status grn_evolution_destroy(grn_evolution *evo);
 

@@ -188,3 +188,82 @@ def test_pipelined_generations_match_synchronous():
         assert [x[k] for x in s1] == [x[k] for x in s2], k
     for a, b in zip(m1, m2):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+
+
+def _populations(evo):
+    return [evo.individual(d, i) for d in range(EVO["n_demes"]) for i in range(EVO["deme_size"])]
+
+
+def _same_populations(a, b):
+    return len(a) == len(b) and all(
+        np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1]) and x[2] == y[2] and
+        x[3] == y[3] for x, y in zip(a, b))
+
+
+def test_checkpoint_restore_continues_the_run_exactly(built_libs):
+    """A search restored from a checkpoint of generation 2 of another run
+    (created with a different seed) goes through generations 3-6 exactly as
+    the original did: populations, errors and statistics, migrations
+    included."""
+    evo = grn.Evolution(dict(EVO, seed=17), 2, calculator=OracleCalculator(SIM))
+    for _ in range(3):
+        evo.step()
+    state = evo.checkpoint()
+    tail = [evo.step() for _ in range(4)]
+    want = _populations(evo)
+    evo2 = grn.Evolution(dict(EVO, seed=99), 2, calculator=OracleCalculator(SIM))
+    evo2.restore(state)
+    tail2 = [evo2.step() for _ in range(4)]
+    keys = ("generation", "n_evaluated", "best_error", "best_complexity", "mean_error",
+            "migrated")
+    assert [[s[k] for k in keys] for s in tail2] == [[s[k] for k in keys] for s in tail]
+    assert _same_populations(_populations(evo2), want)
+    # the checkpoint of the restored search at the same point equals the original's
+    assert evo2.checkpoint() == evo.checkpoint()
+    evo.close()
+    evo2.close()
+
+
+def test_restore_rejects_foreign_or_damaged_checkpoints(built_libs):
+    evo = grn.Evolution(dict(EVO, seed=17), 2, calculator=OracleCalculator(SIM))
+    evo.step()
+    state = evo.checkpoint()
+    before = _populations(evo)
+    for bad in (state[:-1], state + b"x", b"GRNEVOCK" + state[8:20], b"x" * 64,
+                state[:8] + b"\x02" + state[9:]):
+        with pytest.raises(grn.GrnError):
+            evo.restore(bad)
+    other = grn.Evolution(dict(EVO, seed=17, deme_size=12), 2, calculator=OracleCalculator(SIM))
+    with pytest.raises(grn.GrnError):
+        other.restore(state)
+    assert _same_populations(_populations(evo), before)  # a failed restore changes nothing
+    evo.close()
+    other.close()
+
+
+@pytest.mark.gpu
+def test_checkpoint_of_a_pipelined_search():
+    """A pipelined search holds children in flight and cannot be
+    checkpointed; switched back to synchronous mode (which drops them) it
+    can, and a restored copy continues exactly like it on the GPU
+    evaluator."""
+    sim = dict(SIM, dim_x=16, dim_y=16, num_sim_steps=60)
+    init, tgt = _experiments(sim)
+    with grn.Evaluator(sim) as ev:
+        ev.set_experiments(init, tgt)
+        p = dict(EVO, deme_size=32, n_max_products=8, n_max_links=24, seed=37)
+        evo = grn.Evolution(p, 2, evaluator=ev)
+        evo.set_pipeline(True)
+        for _ in range(3):
+            evo.step()
+        with pytest.raises(grn.GrnError):
+            evo.checkpoint()
+        evo.set_pipeline(False)
+        state = evo.checkpoint()
+        evo2 = grn.Evolution(dict(p, seed=1), 2, evaluator=ev)
+        evo2.restore(state)
+        a = [evo.step()["best_error"] for _ in range(3)]
+        b = [evo2.step()["best_error"] for _ in range(3)]
+        assert a == b and evo.checkpoint() == evo2.checkpoint()
+        evo.close()
+        evo2.close()

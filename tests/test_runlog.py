@@ -49,3 +49,28 @@ def test_resume_rejects_empty_population(built_libs):
     except grn.GrnError as e:
         assert "MODEL" in str(e)
     evo.close()
+
+
+def test_resume_from_a_recorded_checkpoint_is_exact(built_libs, tmp_path):
+    """record_generation(checkpoint=True) stores the search's exact state;
+    resume then continues as the recorded run did."""
+    evo = grn.Evolution(dict(EVO, seed=23), 2, calculator=OracleCalculator(SIM))
+    log = runlog.RunLog(str(tmp_path / "run.db"))
+    for _ in range(3):
+        st = evo.step()
+        log.record_generation(evo, EVO["n_demes"], EVO["deme_size"], st["generation"],
+                              checkpoint=(st["generation"] == 1))
+    tail = [evo.step() for _ in range(2)]  # generations 3 and 4
+    evo2 = grn.Evolution(dict(EVO, seed=5), 2, calculator=OracleCalculator(SIM))
+    log.resume(evo2, 1)
+    tail2 = [evo2.step() for _ in range(3)][1:]  # generations 2, 3, 4
+    assert [s["generation"] for s in tail2] == [s["generation"] for s in tail] == [3, 4]
+    assert [s["mean_error"] for s in tail2] == [s["mean_error"] for s in tail]
+    for d in range(EVO["n_demes"]):
+        for i in range(EVO["deme_size"]):
+            a, b = evo.individual(d, i), evo2.individual(d, i)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    log.close()
+    evo.close()
+    evo2.close()
+
