@@ -585,6 +585,9 @@ def main():
     n = batch.n_models
     ev = grn.Evaluator(params, device=local)
     ev.set_experiments(init, tgt)
+    if world > 1:  # the ranks of this node share its cores for compiling batches
+        local_world = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        ev.set_host_threads(max(1, (os.cpu_count() or 1) // local_world))
     if args.schedule != "auto":  # a fixed schedule: no autotuning launches (profiling)
         ev.set_schedule({v: k for k, v in grn.SCHEDULE_NAMES.items()}[args.schedule])
     pk = ev.pack(batch)

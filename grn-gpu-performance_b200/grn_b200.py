@@ -125,6 +125,7 @@ _SIGNATURES = {
     "grn_set_autotune": ([_P, _I], _I),
     "grn_autotune_report": ([_P, _P, _I], _I),
     "grn_set_graphs": ([_P, _I], _I),
+    "grn_set_host_threads": ([_P, _I], _I),
     "grn_set_test_hooks": ([_P, _I], _I),
     "grn_set_experiments": ([_P, _I, _P, _P], _I),
     "grn_set_experiments_rgb": ([_P, _I, _P, _P], _I),
@@ -379,6 +380,10 @@ class Evaluator:
         buf = ctypes.create_string_buffer(8192)
         self.lib.grn_autotune_report(self.ctx, buf, len(buf))
         return buf.value.decode()
+
+    def set_host_threads(self, n_threads):
+        """Threads that compile a batch (0: the CPUs this process may use)."""
+        _check(self.lib.grn_set_host_threads(self.ctx, int(n_threads)), self.ctx)
 
     def set_autotune(self, enable=True):
         _check(self.lib.grn_set_autotune(self.ctx, int(bool(enable))), self.ctx)

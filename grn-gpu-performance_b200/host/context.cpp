@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include <sched.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -81,6 +83,7 @@ struct grn_ctx {
   int forced_cluster = 0;
   int test_hooks = 0;   // grn_set_test_hooks
   bool graphs = false;  // evaluations replay one CUDA graph per job
+  int host_threads = 0;  // threads compiling a batch (0: the CPUs this process may use)
   // Measured autotuning of GRN_SCHEDULE_AUTO: the fastest plan timed on a
   // sample of the first batch of each shape, by (W, H, max genes, max links,
   // experiments, fast path, batch-size bucket).
@@ -207,8 +210,17 @@ grn_status check_batch(grn_ctx *ctx, const grn_model_batch *b) {
   return GRN_OK;
 }
 
-int host_threads() {
-  unsigned n = std::thread::hardware_concurrency();
+// Threads that compile a batch: the context's setting, else the CPUs this
+// process may run on (its affinity mask: several ranks of one node each get
+// their share when a launcher pins them).
+int host_threads(const grn_ctx *ctx) {
+  if (ctx->host_threads > 0) return ctx->host_threads;
+  cpu_set_t set;
+  if (sched_getaffinity(0, sizeof set, &set) == 0) {
+    const int n = CPU_COUNT(&set);
+    if (n > 0) return n;
+  }
+  const unsigned n = std::thread::hardware_concurrency();
   return n ? (int)n : 1;
 }
 
@@ -771,7 +783,7 @@ grn_status enqueue_job(grn_ctx *ctx, Job *j, const grn_model_batch *batch,
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
                       (float)ctx->p.dt, ctx->p.num_sim_steps,
-                      host_threads(), &ph, &err);
+                      host_threads(ctx), &ph, &err);
   if (s != GRN_OK) return fail(ctx, s, err);
   auto t1 = std::chrono::steady_clock::now();
   if (n == 0) return GRN_OK;
@@ -967,6 +979,12 @@ grn_status grn_set_test_hooks(grn_ctx *ctx, int hooks) {
   return GRN_OK;
 }
 
+grn_status grn_set_host_threads(grn_ctx *ctx, int n_threads) {
+  if (!ctx || n_threads < 0) return GRN_ERR_INVALID_ARGUMENT;
+  ctx->host_threads = n_threads;
+  return GRN_OK;
+}
+
 grn_status grn_set_graphs(grn_ctx *ctx, int enable) {
   if (!ctx) return GRN_ERR_INVALID_ARGUMENT;
   ctx->graphs = enable != 0;
@@ -1095,7 +1113,7 @@ grn_status grn_evaluate_states(grn_ctx *ctx, const grn_model_batch *batch, const
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
                       (float)ctx->p.dt, ctx->p.num_sim_steps,
-                      host_threads(), &ph, &err);
+                      host_threads(ctx), &ph, &err);
   if (s != GRN_OK) return fail(ctx, s, err);
   Job &j = ctx->sync_job;
   const size_t wb = ph.words.size() * sizeof(uint4), ob = n * sizeof(int32_t);
@@ -1223,7 +1241,7 @@ grn_status grn_pack(grn_ctx *ctx, const grn_model_batch *batch, grn_packed **out
   std::string err;
   s = grn::pack_batch(batch, ctx->p.n_input_morphogens + ctx->p.n_target_morphogens,
                       (float)ctx->p.dt, ctx->p.num_sim_steps,
-                      host_threads(), &pk->host, &err);
+                      host_threads(ctx), &pk->host, &err);
   if (s != GRN_OK) {
     delete pk;
     return fail(ctx, s, err);

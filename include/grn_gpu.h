@@ -236,6 +236,11 @@ grn_status grn_autotune_report(const grn_ctx *ctx, char *buf, int buf_len);
  * once without a graph.  Off by default. */
 grn_status grn_set_graphs(grn_ctx *ctx, int enable);
 
+/* Host threads that compile a batch into its packed form (at most 16 are
+ * used).  0 (the default): as many as the CPUs this process may run on.
+ * Several processes of one node (one per GPU) each want their share. */
+grn_status grn_set_host_threads(grn_ctx *ctx, int n_threads);
+
 /* Tests of the error paths only.  GRN_TEST_WITHHOLD_BAND_COPY: the
  * streaming schedule never issues the bulk copy of each step's second band,
  * so the kernel's bounded wait for it runs out (about one second per model),

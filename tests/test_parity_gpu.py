@@ -688,3 +688,17 @@ def test_full_headline_workload_properties():
     sub = batch.subset(idx)
     oe, oraw, _ = oracle.evaluate_batch(params, init, tgt, sub)
     assert_raw_close(raw1[idx], oraw, what="headline sample")
+
+
+def test_host_thread_count_does_not_change_results():
+    """Batches compiled by one host thread or by many give the same errors
+    bit for bit (the record order is the cost order either way)."""
+    params, batch, init, tgt = synth.workload("uneven_64x64", seed=43, n_models=600, steps=30)
+    out = []
+    for n in (1, 0, 5):
+        with grn.Evaluator(params) as ev:
+            ev.set_experiments(init, tgt)
+            ev.set_host_threads(n)
+            out.append(ev.evaluate_batch(batch)[1])
+    np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_array_equal(out[0], out[2])
