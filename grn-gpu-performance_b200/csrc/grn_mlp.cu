@@ -161,7 +161,8 @@ constexpr int kLossThreads = 1024;
 
 __global__ void __launch_bounds__(kLossThreads)
     loss_kernel(int B, const float *__restrict__ y, const float *__restrict__ t,
-                float *__restrict__ dy, double *__restrict__ loss, float *__restrict__ db) {
+                float *__restrict__ dy, double *__restrict__ loss, float *__restrict__ db,
+                int *__restrict__ adam_step) {
   __shared__ double part[kLossThreads];
   __shared__ float dpart[kLossThreads];
   double s = 0.0;
@@ -189,6 +190,7 @@ __global__ void __launch_bounds__(kLossThreads)
     loss[0] = l;
     loss[1] += l;
     db[0] = dpart[0];
+    if (adam_step) *adam_step += 1;  // the Adam step this minibatch takes
   }
 }
 
@@ -331,13 +333,16 @@ __global__ void __launch_bounds__(256) row_sums_kernel(const RowSumJobs jobs, in
   if (threadIdx.x == 0) jb.out[blockIdx.x] = part[0];
 }
 
-// Adam on FP32 master weights; refreshes the BF16 copy and the transposed
-// BF16 copies of the square matrices listed in tr.
+// Adam on FP32 master weights, step t = *adam_step (device memory, so that
+// a captured training step replays as is); refreshes the BF16 copy and the
+// transposed BF16 copies of the square matrices listed in tr.
 __global__ void adam_kernel(int n, float *w, const float *g, float *m, float *v, float lr,
-                            float b1, float b2, float eps, float c1, float c2,
+                            float b1, float b2, float eps, const int *adam_step,
                             __nv_bfloat16 *wb, const MlpTransposed tr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const float t = (float)*adam_step;
+  const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
   const float gi = g[i];
   const float mi = b1 * m[i] + (1.0f - b1) * gi;
   const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
@@ -387,8 +392,8 @@ cudaError_t mlp_output_forward(int B, int K, const __nv_bfloat16 *h, const float
 }
 
 cudaError_t mlp_loss(int B, const float *y, const float *t, float *dy, double *loss, float *db,
-                     cudaStream_t st) {
-  loss_kernel<<<1, kLossThreads, 0, st>>>(B, y, t, dy, loss, db);
+                     int *adam_step, cudaStream_t st) {
+  loss_kernel<<<1, kLossThreads, 0, st>>>(B, y, t, dy, loss, db, adam_step);
   return cudaGetLastError();
 }
 
@@ -411,10 +416,10 @@ cudaError_t mlp_row_sums(int n_jobs, const MlpRowSum *jobs, int rows, int cols, 
 }
 
 cudaError_t mlp_adam(int n, float *w, const float *g, float *m, float *v, float lr, float b1,
-                     float b2, float eps, int t, __nv_bfloat16 *wb, const MlpTransposed &tr,
-                     cudaStream_t st) {
-  const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
-  adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, g, m, v, lr, b1, b2, eps, c1, c2, wb, tr);
+                     float b2, float eps, const int *adam_step, __nv_bfloat16 *wb,
+                     const MlpTransposed &tr, cudaStream_t st) {
+  adam_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, g, m, v, lr, b1, b2, eps, adam_step, wb,
+                                               tr);
   return cudaGetLastError();
 }
 

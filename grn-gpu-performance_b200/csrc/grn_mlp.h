@@ -52,9 +52,10 @@ cudaError_t mlp_gemm_tc(const MlpGemm &p, float *work, size_t work_elems, int *e
 cudaError_t mlp_output_forward(int B, int K, const __nv_bfloat16 *h, const float *w,
                                const float *b0, float *y, cudaStream_t st);
 // dy = 2 (y - t) / B; loss[0] = mean (y - t)^2, loss[1] += loss[0];
-// db[0] = sum dy (the output bias gradient).
+// db[0] = sum dy (the output bias gradient); *adam_step += 1 unless null
+// (a training step's count of Adam steps, read by mlp_adam).
 cudaError_t mlp_loss(int B, const float *y, const float *t, float *dy, double *loss, float *db,
-                     cudaStream_t st);
+                     int *adam_step, cudaStream_t st);
 // dz[b][k] = h[b][k] > 0 ? dy[b] w[k] : 0 (BF16), and its transpose dzT[k][b].
 cudaError_t mlp_output_backward(int B, int K, const __nv_bfloat16 *h, const float *w,
                                 const float *dy, __nv_bfloat16 *dz, __nv_bfloat16 *dzT,
@@ -75,11 +76,12 @@ struct MlpTransposed {
   __nv_bfloat16 *dst[2];
   int n;
 };
-// One Adam step on the FP32 parameters w (moments m, v; step t), refreshing
-// their BF16 copy wb and the transposed copies of tr.
+// One Adam step on the FP32 parameters w (moments m, v; step number
+// *adam_step, in device memory), refreshing their BF16 copy wb and the
+// transposed copies of tr.
 cudaError_t mlp_adam(int n, float *w, const float *g, float *m, float *v, float lr, float b1,
-                     float b2, float eps, int t, __nv_bfloat16 *wb, const MlpTransposed &tr,
-                     cudaStream_t st);
+                     float b2, float eps, const int *adam_step, __nv_bfloat16 *wb,
+                     const MlpTransposed &tr, cudaStream_t st);
 cudaError_t mlp_to_bf16(int n, const float *x, __nv_bfloat16 *y, cudaStream_t st);
 // dst[c][r] = src[r][c] for a rows x cols BF16 matrix.
 cudaError_t mlp_transpose(int rows, int cols, const __nv_bfloat16 *src, int64_t lds,

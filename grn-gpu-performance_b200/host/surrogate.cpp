@@ -64,7 +64,14 @@ struct grn_surrogate {
   __nv_bfloat16 *dx = nullptr;
   float *dt = nullptr;
   int step = 0;
+  int *d_step = nullptr;   // Adam steps taken (device; the captured step reads it)
   std::mt19937_64 rng;
+  // One training step (forward, backward, Adam) captured as a CUDA graph for
+  // this batch size, learning rate and tensor-core path.
+  cudaGraphExec_t train_exec = nullptr;
+  int graph_B = 0;
+  float graph_lr = 0;
+  bool graph_tc = true;
   bool tcgen05 = true;     // GEMMs on tcgen05 (else mma.sync)
   int *d_err = nullptr;    // set by a tcgen05 GEMM whose wait timed out
 };
@@ -125,12 +132,12 @@ grn_status forward(grn_surrogate *s, int B, bool train) {
 }
 
 // Loss and gradients of a minibatch already in s->x / s->xT / s->t (after
-// forward with train set).
-grn_status backward(grn_surrogate *s, int B) {
+// forward with train set); `adam` counts the Adam step that follows.
+grn_status backward(grn_surrogate *s, int B, bool adam) {
   using namespace grn;
   cudaStream_t st = s->st;
   const int64_t T = s->bmax;
-  GRN_CK(mlp_loss(B, s->y, s->t, s->dy, s->loss, s->g + kB4, st));
+  GRN_CK(mlp_loss(B, s->y, s->t, s->dy, s->loss, s->g + kB4, adam ? s->d_step : nullptr, st));
   GRN_CK(mlp_output_backward(B, kH, s->h3, s->w + kW4, s->dy, s->dz3, s->dz3T, T, st));
   // Per hidden layer l = 3, 2, 1: dW_l = dZ_l^T H_(l-1) (K = the batch, from
   // the transposed copies), and for l > 1 dZ_(l-1) = (dZ_l W_l) * [H_(l-1) > 0].
@@ -175,17 +182,59 @@ grn_status transpose_weights(grn_surrogate *s) {
   return GRN_OK;
 }
 
+// Forward, backward and Adam on the minibatch in s->x / s->xT / s->t.
+grn_status train_step_body(grn_surrogate *s, int B, float lr) {
+  grn_status st = forward(s, B, true);
+  if (st == GRN_OK) st = backward(s, B, true);
+  if (st != GRN_OK) return st;
+  const grn::MlpTransposed tr{{kW2, kW3}, {s->w2t, s->w3t}, kH};
+  GRN_CK(grn::mlp_adam((int)kP, s->w, s->g, s->m, s->v, lr, 0.9f, 0.999f, 1e-8f, s->d_step,
+                       s->wb, tr, s->st));
+  return GRN_OK;
+}
+
+void drop_train_graph(grn_surrogate *s) {
+  if (s->train_exec) cudaGraphExecDestroy(s->train_exec);
+  s->train_exec = nullptr;
+}
+
+// One training step.  The first step of a (batch size, learning rate,
+// tensor-core path) runs its 16 launches directly -- which also loads every
+// kernel's module -- and is then captured as a graph; later steps replay it
+// (the kernels' arguments do not change; the Adam step count is read from
+// device memory).
+grn_status train_step(grn_surrogate *s, int B, float lr) {
+  if (s->train_exec && s->graph_B == B && s->graph_lr == lr && s->graph_tc == s->tcgen05) {
+    GRN_CK(cudaGraphLaunch(s->train_exec, s->st));
+    return GRN_OK;
+  }
+  drop_train_graph(s);
+  grn_status st = train_step_body(s, B, lr);
+  if (st != GRN_OK) return st;
+  GRN_CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeRelaxed));
+  st = train_step_body(s, B, lr);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s->st, &graph);
+  cudaError_t ei = cudaSuccess;
+  if (st == GRN_OK && ec == cudaSuccess) ei = cudaGraphInstantiate(&s->train_exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (st != GRN_OK || ec != cudaSuccess || ei != cudaSuccess) {
+    s->train_exec = nullptr;
+    cudaGetLastError();
+    return st != GRN_OK ? st : GRN_ERR_CUDA;
+  }
+  s->graph_B = B;
+  s->graph_lr = lr;
+  s->graph_tc = s->tcgen05;
+  return GRN_OK;
+}
+
 // One Adam step on the training-set rows d_idx[0..B) (device indices).
 grn_status train_minibatch(grn_surrogate *s, const int32_t *d_idx, int B, float lr) {
   GRN_CK(grn::mlp_gather_rows(B, kF, d_idx, s->dx, s->dt, s->x, s->t, s->xT, s->bmax, s->st));
-  grn_status st = forward(s, B, true);
-  if (st == GRN_OK) st = backward(s, B);
-  if (st != GRN_OK) return st;
-  s->step += 1;
-  const grn::MlpTransposed tr{{kW2, kW3}, {s->w2t, s->w3t}, kH};
-  GRN_CK(grn::mlp_adam((int)kP, s->w, s->g, s->m, s->v, lr, 0.9f, 0.999f, 1e-8f, s->step, s->wb,
-                       tr, s->st));
-  return GRN_OK;
+  const grn_status st = train_step(s, B, lr);
+  if (st == GRN_OK) s->step += 1;
+  return st;
 }
 
 // Runs minibatch i on the sizes[i] training-set rows that follow in idx.
@@ -321,6 +370,8 @@ grn_status grn_surrogate_create(int device, uint64_t seed, int capacity, grn_sur
   alloc((void **)&s->dt, (size_t)capacity * 4);
   alloc((void **)&s->d_err, sizeof(int));
   if (ok && cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess) ok = false;
+  alloc((void **)&s->d_step, sizeof(int));
+  if (ok && cudaMemset(s->d_step, 0, sizeof(int)) != cudaSuccess) ok = false;
   if (!ok) {
     grn_surrogate_destroy(s);
     return GRN_ERR_OUT_OF_MEMORY;
@@ -348,13 +399,14 @@ grn_status grn_surrogate_destroy(grn_surrogate *s) {
   if (!s) return GRN_OK;
   cudaSetDevice(s->device);
   if (s->st) cudaStreamSynchronize(s->st);
+  drop_train_graph(s);
   for (void *p : {(void *)s->w, (void *)s->g, (void *)s->m, (void *)s->v, (void *)s->wb,
                   (void *)s->w2t, (void *)s->w3t, (void *)s->x, (void *)s->h1, (void *)s->h2,
                   (void *)s->h3, (void *)s->dz1, (void *)s->dz2, (void *)s->dz3, (void *)s->xT,
                   (void *)s->h1T, (void *)s->h2T, (void *)s->h3T, (void *)s->dz1T,
                   (void *)s->dz2T, (void *)s->dz3T, (void *)s->xf, (void *)s->y, (void *)s->t,
                   (void *)s->dy, (void *)s->loss, (void *)s->work, (void *)s->idx, (void *)s->dx,
-                  (void *)s->dt, (void *)s->d_err})
+                  (void *)s->dt, (void *)s->d_err, (void *)s->d_step})
     if (p) cudaFree(p);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
@@ -367,6 +419,7 @@ grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n
   GRN_CK(cudaMemcpyAsync(s->w, params, kP * 4, cudaMemcpyHostToDevice, s->st));
   GRN_CK(cudaMemsetAsync(s->m, 0, kP * 4, s->st));
   GRN_CK(cudaMemsetAsync(s->v, 0, kP * 4, s->st));
+  GRN_CK(cudaMemsetAsync(s->d_step, 0, sizeof(int), s->st));
   GRN_CK(grn::mlp_to_bf16((int)kP, s->w, s->wb, s->st));
   const grn_status ts = transpose_weights(s);
   if (ts != GRN_OK) return ts;
@@ -472,7 +525,7 @@ grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
   if (st != GRN_OK) return st;
   GRN_CK(cudaMemcpyAsync(s->t, log_error, n * 4, cudaMemcpyHostToDevice, s->st));
   st = forward(s, n, true);
-  if (st == GRN_OK) st = backward(s, n);
+  if (st == GRN_OK) st = backward(s, n, false);
   if (st != GRN_OK) return st;
   GRN_CK(cudaMemcpyAsync(grads, s->g, kP * 4, cudaMemcpyDeviceToHost, s->st));
   double l = 0;
