@@ -172,6 +172,8 @@ _SIGNATURES = {
     "grn_surrogate_train_batches": ([_P, _I, _I, ctypes.c_float, ctypes.POINTER(_D)], _I),
     "grn_surrogate_predict": ([_P, _P, _I, _P], _I),
     "grn_surrogate_use_tcgen05": ([_P, _I], _I),
+    "grn_surrogate_checkpoint": ([_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], _I),
+    "grn_surrogate_restore": ([_P, _P, ctypes.c_size_t], _I),
     "grn_surrogate_params": ([_P, _P, _I], _I),
     "grn_surrogate_set_params": ([_P, _P, _I], _I),
     "grn_surrogate_gradients": ([_P, _P, _P, _I, _P, ctypes.POINTER(_D)], _I),
@@ -736,6 +738,17 @@ class Surrogate:
 
     def use_tcgen05(self, enable=True):
         _check(self.lib.grn_surrogate_use_tcgen05(self.handle, int(bool(enable))))
+
+    def checkpoint(self):
+        """Weights, optimiser state and training set as bytes."""
+        n = ctypes.c_size_t()
+        _check(self.lib.grn_surrogate_checkpoint(self.handle, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(self.lib.grn_surrogate_checkpoint(self.handle, buf, n.value, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def restore(self, state):
+        _check(self.lib.grn_surrogate_restore(self.handle, state, len(state)))
 
     def train_batches(self, n_batches, batch_size=512, lr=1e-3):
         loss = ctypes.c_double()

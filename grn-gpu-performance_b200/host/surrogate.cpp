@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <random>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -508,6 +509,101 @@ grn_status grn_surrogate_predict(grn_surrogate *s, const float *features, int n,
     GRN_CK(cudaStreamSynchronize(s->st));
   }
   return check_err(s);
+}
+
+// Checkpoint layout (host byte order): magic, version, parameter count,
+// capacity, count, head, host step, the sampling RNG (std::mt19937_64 text
+// form), then the FP32 weights, Adam's two moments and step, and the
+// training set's first `count` rows (BF16 features, FP32 targets) when the
+// ring has not wrapped, else all `capacity` rows.
+grn_status grn_surrogate_checkpoint(grn_surrogate *s, void *buf, size_t cap, size_t *size) {
+  if (!s || !size) return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  const int rows = s->count < s->cap ? s->count : s->cap;
+  std::ostringstream rng_text;
+  rng_text << s->rng;
+  const std::string rt = rng_text.str();
+  const size_t head_bytes = 8 + 4 * 7 + 8 + rt.size();
+  const size_t total = head_bytes + 3 * (size_t)kP * 4 + 4 + (size_t)rows * (kF * 2 + 4);
+  *size = total;
+  if (!buf) return GRN_OK;
+  if (cap < total) return GRN_ERR_CAPACITY;
+  char *o = static_cast<char *>(buf);
+  auto put = [&](const void *p, size_t n) {
+    std::memcpy(o, p, n);
+    o += n;
+  };
+  const uint32_t version = 1;
+  const int32_t hdr[6] = {(int32_t)kP, s->cap, s->count, s->head, s->step, s->tcgen05 ? 1 : 0};
+  const uint64_t rlen = rt.size();
+  put("GRNSURCK", 8);
+  put(&version, 4);
+  put(hdr, sizeof hdr);
+  put(&rlen, 8);
+  put(rt.data(), rt.size());
+  GRN_CK(cudaMemcpyAsync(o, s->w, kP * 4, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaMemcpyAsync(o + kP * 4, s->m, kP * 4, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaMemcpyAsync(o + 2 * kP * 4, s->v, kP * 4, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaMemcpyAsync(o + 3 * kP * 4, s->d_step, 4, cudaMemcpyDeviceToHost, s->st));
+  char *d = o + 3 * kP * 4 + 4;
+  GRN_CK(cudaMemcpyAsync(d, s->dx, (size_t)rows * kF * 2, cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaMemcpyAsync(d + (size_t)rows * kF * 2, s->dt, (size_t)rows * 4,
+                         cudaMemcpyDeviceToHost, s->st));
+  GRN_CK(cudaStreamSynchronize(s->st));
+  return GRN_OK;
+}
+
+grn_status grn_surrogate_restore(grn_surrogate *s, const void *buf, size_t size) {
+  if (!s || !buf) return GRN_ERR_INVALID_ARGUMENT;
+  const char *p = static_cast<const char *>(buf), *end = p + size;
+  auto get = [&](void *v, size_t n) {
+    if ((size_t)(end - p) < n) return false;
+    std::memcpy(v, p, n);
+    p += n;
+    return true;
+  };
+  char magic[8];
+  uint32_t version = 0;
+  int32_t hdr[6];
+  uint64_t rlen = 0;
+  if (!get(magic, 8) || std::memcmp(magic, "GRNSURCK", 8) != 0 || !get(&version, 4) ||
+      version != 1 || !get(hdr, sizeof hdr) || !get(&rlen, 8) || rlen > (1u << 16) ||
+      (size_t)(end - p) < rlen)
+    return GRN_ERR_INVALID_ARGUMENT;
+  const int cap = hdr[1], count = hdr[2], head = hdr[3];
+  if (hdr[0] != (int32_t)kP || cap != s->cap || count < 0 || count > cap || head < 0 ||
+      head >= cap)
+    return GRN_ERR_INVALID_ARGUMENT;
+  std::mt19937_64 rng;
+  {
+    std::istringstream i(std::string(p, (size_t)rlen));
+    if (!(i >> rng)) return GRN_ERR_INVALID_ARGUMENT;
+  }
+  p += rlen;
+  const int rows = count < cap ? count : cap;
+  if ((size_t)(end - p) != 3 * (size_t)kP * 4 + 4 + (size_t)rows * (kF * 2 + 4))
+    return GRN_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(s->device);
+  GRN_CK(cudaStreamSynchronize(s->st));
+  drop_train_graph(s);
+  GRN_CK(cudaMemcpyAsync(s->w, p, kP * 4, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaMemcpyAsync(s->m, p + kP * 4, kP * 4, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaMemcpyAsync(s->v, p + 2 * kP * 4, kP * 4, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaMemcpyAsync(s->d_step, p + 3 * kP * 4, 4, cudaMemcpyHostToDevice, s->st));
+  const char *d = p + 3 * kP * 4 + 4;
+  GRN_CK(cudaMemcpyAsync(s->dx, d, (size_t)rows * kF * 2, cudaMemcpyHostToDevice, s->st));
+  GRN_CK(cudaMemcpyAsync(s->dt, d + (size_t)rows * kF * 2, (size_t)rows * 4,
+                         cudaMemcpyHostToDevice, s->st));
+  GRN_CK(grn::mlp_to_bf16((int)kP, s->w, s->wb, s->st));
+  const grn_status ts = transpose_weights(s);
+  if (ts != GRN_OK) return ts;
+  GRN_CK(cudaStreamSynchronize(s->st));
+  s->count = count;
+  s->head = head;
+  s->step = hdr[4];
+  s->tcgen05 = hdr[5] != 0;
+  s->rng = rng;
+  return GRN_OK;
 }
 
 grn_status grn_surrogate_use_tcgen05(grn_surrogate *s, int enable) {

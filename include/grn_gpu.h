@@ -541,7 +541,7 @@ grn_status grn_evolution_set_generation(grn_evolution *evo, int generation);
  * populations only).  grn_evolution_restore into a search created with the
  * same parameters continues exactly as the checkpointed search would have,
  * given a deterministic evaluator.  An attached surrogate is not part of the
- * checkpoint (save it with grn_surrogate_params).
+ * checkpoint (grn_surrogate_checkpoint saves it).
  * grn_evolution_checkpoint sets *size to the byte count and writes the bytes
  * when buf is not NULL (GRN_ERR_CAPACITY if cap is smaller).  A pipelined
  * search with children in flight cannot be checkpointed
@@ -608,6 +608,16 @@ grn_status grn_surrogate_set_params(grn_surrogate *s, const float *params, int n
  * GRN_ERR_KERNEL from a surrogate call means a tcgen05 GEMM's bounded wait
  * for the tensor core ran out. */
 grn_status grn_surrogate_use_tcgen05(grn_surrogate *s, int enable);
+/* Checkpoint of a surrogate as an opaque byte string: weights, Adam's
+ * moments and step, the training set (the rows it holds), the minibatch
+ * sampling state and the tensor-core path.  Restored into a surrogate of the
+ * same capacity it trains and predicts exactly as the original would have;
+ * with grn_evolution_checkpoint it lets a screened search resume exactly.
+ * grn_surrogate_checkpoint sets *size and writes the bytes when buf is not
+ * NULL (GRN_ERR_CAPACITY if cap is smaller); grn_surrogate_restore rejects
+ * other layouts or capacities with GRN_ERR_INVALID_ARGUMENT. */
+grn_status grn_surrogate_checkpoint(grn_surrogate *s, void *buf, size_t cap, size_t *size);
+grn_status grn_surrogate_restore(grn_surrogate *s, const void *buf, size_t size);
 /* Mean squared loss and its parameter gradients on n pairs, no update. */
 grn_status grn_surrogate_gradients(grn_surrogate *s, const float *features,
                                    const float *log_error, int n, float *grads, double *loss);

@@ -376,3 +376,46 @@ def test_surrogate_tiny_and_ragged_batches(built_libs):
         for name, _ in mlp_ref.SHAPES:
             assert np.linalg.norm(gb[name] - rb[name]) <= 5e-3 * np.linalg.norm(rb[name]) + 1e-7, \
                 (n, name)
+
+
+@pytest.mark.gpu
+def test_screened_search_resumes_exactly(built_libs):
+    """A surrogate-screened search checkpointed after generation 7 (search
+    and surrogate) and restored into new objects with other seeds goes on
+    exactly like the original: the same screening, simulations, losses and
+    best errors."""
+    params = dict(dim_x=16, dim_y=16, n_input_morphogens=1, n_target_morphogens=1,
+                  num_sim_steps=100, error_precision=8, fitness_kind=0, dt=0.1, min_conc=0.0,
+                  min_conc_change=0.0, dist_error_threshold=0.05)
+    wl = dict(synth.WORKLOADS["uneven_64x64"], W=16, H=16, n_exp=1)
+    init, tgt = synth.experiments(wl, 12)
+    evo_p = dict(n_demes=4, deme_size=64, migration_period=5, n_max_products=6, n_max_links=12,
+                 n_host_threads=2, seed=9)
+    sur_kw = dict(simulate_fraction=0.25, min_train_pairs=512, batches_per_generation=8,
+                  batch_size=128)
+    keys = ("generation", "n_evaluated", "n_screened", "best_error", "mean_error",
+            "surrogate_loss", "n_clones")
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments(init, tgt)
+        evo = grn.Evolution(evo_p, 2, evaluator=ev)
+        sur = grn.Surrogate(seed=4, capacity=5000)
+        evo.set_surrogate(sur, **sur_kw)
+        for _ in range(8):
+            evo.step()
+        state, sstate = evo.checkpoint(), sur.checkpoint()
+        tail = [evo.step() for _ in range(6)]
+        evo2 = grn.Evolution(dict(evo_p, seed=1), 2, evaluator=ev)
+        sur2 = grn.Surrogate(seed=8, capacity=5000)
+        evo2.set_surrogate(sur2, **sur_kw)
+        evo2.restore(state)
+        sur2.restore(sstate)
+        tail2 = [evo2.step() for _ in range(6)]
+        assert sum(s["n_screened"] for s in tail) > 0
+        assert [[s[k] for k in keys] for s in tail2] == [[s[k] for k in keys] for s in tail]
+        assert evo2.checkpoint() == evo.checkpoint()
+        with pytest.raises(grn.GrnError):
+            grn.Surrogate(seed=8, capacity=4000).restore(sstate)  # another capacity
+        for e in (evo, evo2):
+            e.close()
+        for s in (sur, sur2):
+            s.close()
