@@ -26,7 +26,7 @@ CREATE TABLE IF NOT EXISTS Generation (
 CREATE TABLE IF NOT EXISTS GenerationIndividual (
   Generation INTEGER NOT NULL, Individual INTEGER NOT NULL, Position INTEGER NOT NULL);
 CREATE TABLE IF NOT EXISTS SearchCheckpoint (
-  Ind INTEGER PRIMARY KEY, State BLOB NOT NULL);
+  Ind INTEGER PRIMARY KEY, State BLOB NOT NULL, Surrogate BLOB);
 """
 
 
@@ -45,12 +45,13 @@ class RunLog:
         self.db.close()
 
     def record_generation(self, evo, n_demes, deme_size, generation, time_s=0.0,
-                          checkpoint=False):
+                          checkpoint=False, surrogate=None):
         """One Generation row per deme (its error and complexity statistics,
         Generation::submit's values) plus its individuals; with `checkpoint`
         also the search's exact state (grn_evolution_checkpoint, a table the
         reference does not have), from which resume continues the run as it
-        would have gone on."""
+        would have gone on; `surrogate` (the search's screen, if any) is
+        checkpointed with it."""
         cur = self.db.cursor()
         for d in range(n_demes):
             inds = [evo.individual(d, i) for i in range(deme_size)]
@@ -71,8 +72,9 @@ class RunLog:
                 cur.execute("INSERT INTO GenerationIndividual VALUES (?,?,?)",
                             (gen_id, cur.lastrowid, pos))
         if checkpoint:
-            cur.execute("INSERT OR REPLACE INTO SearchCheckpoint VALUES (?,?)",
-                        (generation, sqlite3.Binary(evo.checkpoint())))
+            sur = sqlite3.Binary(surrogate.checkpoint()) if surrogate is not None else None
+            cur.execute("INSERT OR REPLACE INTO SearchCheckpoint VALUES (?,?,?)",
+                        (generation, sqlite3.Binary(evo.checkpoint()), sur))
         self.db.commit()
 
     def generations(self):
@@ -93,17 +95,20 @@ class RunLog:
             pop.setdefault(deme, []).append((prods, links, err))
         return pop
 
-    def resume(self, evo, generation):
+    def resume(self, evo, generation, surrogate=None):
         """Loads a recorded generation into `evo` (same deme count and size).
         Where the generation was recorded with its checkpoint, the search
         continues exactly as the recorded run did (given a deterministic
         evaluator).  Otherwise only the populations and their errors load,
         and the search's random state starts afresh, so the continuation
-        differs from the original run's."""
-        row = self.db.execute("SELECT State FROM SearchCheckpoint WHERE Ind = ?",
+        differs from the original run's.  `surrogate` receives the recorded
+        surrogate state, where there is one."""
+        row = self.db.execute("SELECT State, Surrogate FROM SearchCheckpoint WHERE Ind = ?",
                               (generation,)).fetchone()
         if row is not None:
             evo.restore(bytes(row[0]))
+            if surrogate is not None and row[1] is not None:
+                surrogate.restore(bytes(row[1]))
             return
         for deme, inds in self.load_population(generation).items():
             for i, (prods, links, err) in enumerate(inds):
