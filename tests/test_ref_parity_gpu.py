@@ -137,3 +137,33 @@ def test_cuda_matches_reference_library(name, n_models, kw):
         rounded, raw, _ = ev.evaluate_batch(parsed)
     assert_errors_match(rounded, raw, want, params["error_precision"], name)
     assert_same_ranking(raw, want)
+
+
+@needs_ref
+def test_evolved_island_models_match_reference_library():
+    """Models an island search actually produces -- mutated near-copies that
+    often share a plateau error -- at the island workload's grid and steps
+    (100 x 100, 1500 steps), evaluated with max-error bounds like a search's
+    (some abandoned): the CUDA path against the reference's own code."""
+    wl = synth.WORKLOADS["islands_100x100"]
+    params = dict(synth.sim_params(wl), fitness_kind=0)
+    init, tgt = synth.experiments(wl, 0)
+    ipx = np.stack([ref.encode_rgb(e) for e in init])
+    tpx = np.stack([ref.encode_rgb(e) for e in tgt])
+    with grn.Evaluator(params) as ev:
+        ev.set_experiments_rgb(ipx, tpx)
+        evo = grn.Evolution(dict(n_demes=4, deme_size=64, migration_period=5, n_max_products=8,
+                                 n_max_links=24, n_host_threads=2, seed=3),
+                            wl["n_in"] + wl["n_target"], evaluator=ev)
+        for _ in range(12):
+            evo.step()
+        inds = [evo.individual(d, i) for d in range(4) for i in range(0, 64, 4)]
+        evo.close()
+        texts = [grn.format_model(p, l, 17) for p, l, _, _ in inds]
+        errs = np.array([e for _, _, e, _ in inds])
+        me = errs * np.where(np.arange(len(errs)) % 5 == 0, 0.5, 2.0)  # every 5th abandoned
+        batch = ModelBatch.from_models([grn.parse_model(t) for t in texts])
+        rounded, raw, _ = ev.evaluate_batch(batch, me)
+    want = ref.evaluate_texts(params, ipx, tpx, texts, me, n_threads=16)
+    assert (want == 100.0).sum() >= len(texts) // 5 - 1 and (want < 100.0).sum() > 40
+    assert_errors_match(rounded, raw, want, params["error_precision"], "evolved")
