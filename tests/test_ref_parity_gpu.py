@@ -124,6 +124,7 @@ needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref was not 
 @pytest.mark.parametrize("name,n_models,kw", [
     ("small_32x32", 64, dict(fitness=0)),   # the full configuration, reference fitness
     ("uneven_64x64", 48, dict()),           # a sample at the full 2000 steps
+    ("large_256x256", 4, dict(steps=300)),  # the spilled-grid paths (8 genes, dt 0.05)
 ])
 def test_cuda_matches_reference_library(name, n_models, kw):
     params, batch, init, tgt = synth.workload(name, seed=91, n_models=n_models, **kw)
